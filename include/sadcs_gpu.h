@@ -1,0 +1,144 @@
+/*
+ * sadcs_gpu.h - C ABI of libsadcs_gpu.so: suffix array and BWT construction on one NVIDIA B200
+ * (sm_100a), entirely in hand-written CUDA kernels.
+ *
+ * Every entry point here replaces one declaration of the reference's GPU interface,
+ * src/cuda/gpusa.h of acesds/sadcs (cited per function), with plain C types: no references,
+ * overloads, default arguments or enum classes, so cgo, JNI, ctypes or a C++ shim can bind it.
+ * include/gpusa.h is that C++ shim: the reference's exact declarations, inline over these.
+ *
+ * Conventions shared with the reference:
+ *   - The suffix array is divsufsort's: SA[i] is the start of the i-th smallest suffix, byte-wise
+ *     lexicographic, a suffix that is a prefix of another being the smaller.
+ *   - The BWT is divsufsort's/libsais's (src/cpu/dcsort.h:36-40): the BWT of text plus a sentinel,
+ *     without the sentinel; primary is the sentinel's row (row of suffix 0, plus one).
+ *   - Host buffers may be pageable or page-locked (sadcs_gpu_allocate_pinned); page-locked ones
+ *     are copied directly at full link speed.
+ *   - Status codes are GpuStatus's values (gpusa.h:22-27); the message of the last failure on the
+ *     calling thread is sadcs_gpu_last_error().
+ *   - A context serves one thread at a time (gpusa.h:91); different threads use different contexts.
+ *     Contexts are bound to the device that was current when they were created.
+ *
+ * Extensions (marked "no counterpart"): 64-bit sizes with uint32 suffix arrays for texts of 2 GiB
+ * and more (up to 2^32 - 256 bytes), SA and BWT from one construction, device-resident inputs and
+ * outputs on a caller's stream, and the SA-to-BWT gather.
+ */
+#ifndef SADCS_GPU_H
+#define SADCS_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* GpuStatus, gpusa.h:22-27. */
+enum {
+    SADCS_OK = 0,
+    SADCS_UNAVAILABLE = 1,        /* no CUDA device or no usable driver */
+    SADCS_NOT_ENOUGH_MEMORY = 2,  /* the input does not fit in free device memory / the context */
+    SADCS_FAILED = 3              /* a CUDA call failed or an argument is invalid; see sadcs_gpu_last_error() */
+};
+
+/* GpuDevice, gpusa.h:29-35. */
+typedef struct sadcs_gpu_device {
+    char name[256];
+    int32_t compute_major;
+    int32_t compute_minor;
+    int64_t total_bytes;
+    int64_t free_bytes;
+} sadcs_gpu_device;
+
+/* GpuStats, gpusa.h:37-53 (same fields and meaning; bool pinned as int32). Seconds are host
+ * wall-clock around each phase, as in the reference; device_* are CUDA-event times on the stream. */
+typedef struct sadcs_gpu_stats {
+    int64_t device_bytes;       /* peak device memory of the construction */
+    int64_t ranking_bytes;
+    int64_t class_sort_bytes;
+    int64_t merge_bytes;
+    int32_t pinned;             /* the transfers were direct copies of page-locked buffers */
+    int32_t character_passes;
+    int32_t doubling_rounds;
+    int32_t reserved;
+    double setup_seconds;
+    double upload_seconds;
+    double device_seconds;
+    double ranking_seconds;
+    double class_sort_seconds;
+    double merge_seconds;
+    double bwt_seconds;
+    double download_seconds;
+} sadcs_gpu_stats;
+
+typedef struct sadcs_gpu_context sadcs_gpu_context;
+
+/* kGpuMemoryReserve, gpusa.h:82: device memory left free when admitting a construction. */
+int64_t sadcs_gpu_memory_reserve(void);
+
+/* gpuSampleSize, gpusa.h:57-60: sample positions (cover mod 32) in a text of n bytes. */
+int64_t sadcs_gpu_sample_size(int64_t n);
+
+/* gpuQueryDevice, gpusa.h:76: the current CUDA device and its memory. */
+int sadcs_gpu_query_device(sadcs_gpu_device* device);
+
+/* gpuRequiredBytes, gpusa.h:79: peak device memory of a construction of n bytes, -1 if n is out of range. */
+int64_t sadcs_gpu_required_bytes(int64_t n);
+
+/* gpuCreateContext, gpusa.h:93: device memory for inputs of up to capacity bytes, reserved once.
+ * Refuses with SADCS_NOT_ENOUGH_MEMORY, allocating nothing, if the peak plus the reserve exceeds
+ * the free device memory. */
+int sadcs_gpu_create_context(int64_t capacity, sadcs_gpu_context** context);
+
+/* gpuDestroyContext, gpusa.h:96. NULL is ignored. */
+void sadcs_gpu_destroy_context(sadcs_gpu_context* context);
+
+/* gpuSuffixArray, gpusa.h:102-103: the suffix array of text[0, n) into sa[0, n) (int32, so
+ * n <= 2^31 - 1025 as in the reference, src/cpu/dcsort.h:21). context may be NULL: a temporary one
+ * is created. With a context, n above its capacity is refused with SADCS_NOT_ENOUGH_MEMORY and the
+ * context stays usable. stats may be NULL. */
+int sadcs_gpu_suffix_array(sadcs_gpu_context* context, const uint8_t* text, int64_t n, int32_t* sa,
+                           sadcs_gpu_stats* stats);
+
+/* gpuBwt, gpusa.h:108-109: the BWT of text[0, n) into bwt[0, n) and its primary index.
+ * bwt may equal text. */
+int sadcs_gpu_bwt(sadcs_gpu_context* context, const uint8_t* text, int64_t n, uint8_t* bwt, int32_t* primary,
+                  sadcs_gpu_stats* stats);
+
+/* gpuRankSample, gpusa.h:115: ranks[pack(p)] of every sample position p (sadcs_gpu_sample_size(n)
+ * entries): the number of sample suffixes smaller than suffix p. */
+int sadcs_gpu_rank_sample(const uint8_t* text, int64_t n, uint32_t* ranks, sadcs_gpu_stats* stats);
+
+/* gpuAllocatePinned / gpuFreePinned, gpusa.h:120-121. */
+void* sadcs_gpu_allocate_pinned(size_t bytes);
+void sadcs_gpu_free_pinned(void* pointer);
+
+/* gpuLastError, gpusa.h:124: the last failure on this thread, "" if none. */
+const char* sadcs_gpu_last_error(void);
+
+/* ---- extensions -------------------------------------------------------------------------------- */
+
+/* No counterpart: the suffix array (uint32) and/or the BWT of text[0, n) from ONE construction,
+ * host to host, for n up to 2^32 - 256. sa or bwt may be NULL (not both). */
+int sadcs_gpu_build(sadcs_gpu_context* context, const uint8_t* text, int64_t n, uint32_t* sa, uint8_t* bwt,
+                    int64_t* primary, sadcs_gpu_stats* stats);
+
+/* No counterpart: the same with device-resident buffers, on the caller's stream (a cudaStream_t,
+ * NULL for the legacy default stream). d_text holds n bytes; d_sa (4n bytes) and d_bwt (n bytes) are
+ * device outputs, either may be NULL (not both). Returns once the results are complete. */
+int sadcs_gpu_build_device(sadcs_gpu_context* context, const uint8_t* d_text, int64_t n, uint32_t* d_sa,
+                           uint8_t* d_bwt, int64_t* primary, void* stream, sadcs_gpu_stats* stats);
+
+/* No counterpart (the SA-to-BWT gather): d_bwt[0, n) from a device suffix array, in the BWT
+ * convention above; *primary gets the sentinel's row. Device buffers, caller's stream. */
+int sadcs_gpu_bwt_from_sa(const uint8_t* d_text, int64_t n, const uint32_t* d_sa, uint8_t* d_bwt,
+                          int64_t* primary, void* stream);
+
+/* No counterpart: the capacity (bytes of text) of a context. */
+int64_t sadcs_gpu_context_capacity(const sadcs_gpu_context* context);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

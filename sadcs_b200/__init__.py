@@ -1,0 +1,288 @@
+"""sadcs_b200: suffix array and BWT construction on one B200, in hand-written sm_100a CUDA kernels.
+
+The Python side mirrors the reference's GPU interface (src/cuda/gpusa.h of acesds/sadcs) over the
+C ABI of ``lib/libsadcs_gpu.so`` (include/sadcs_gpu.h):
+
+=========================  =====================================  ===========================
+here                       C ABI                                  reference (gpusa.h)
+=========================  =====================================  ===========================
+``query_device()``         ``sadcs_gpu_query_device``             ``gpuQueryDevice`` :76
+``required_bytes(n)``      ``sadcs_gpu_required_bytes``           ``gpuRequiredBytes`` :79
+``sample_size(n)``         ``sadcs_gpu_sample_size``              ``gpuSampleSize`` :57-60
+``Context(capacity)``      ``sadcs_gpu_create/destroy_context``   ``gpuCreateContext`` :93, :96
+``suffix_array(text)``     ``sadcs_gpu_suffix_array``             ``gpuSuffixArray`` :102-103
+``bwt(text)``              ``sadcs_gpu_bwt``                      ``gpuBwt`` :108-109
+``rank_sample(text)``      ``sadcs_gpu_rank_sample``              ``gpuRankSample`` :115
+``allocate_pinned(n)``     ``sadcs_gpu_allocate_pinned``          ``gpuAllocatePinned`` :120
+``build(text)``            ``sadcs_gpu_build``                    (no counterpart: SA + BWT)
+``build_device(...)``      ``sadcs_gpu_build_device``             (no counterpart)
+``bwt_from_sa_device``     ``sadcs_gpu_bwt_from_sa``              (no counterpart)
+=========================  =====================================  ===========================
+
+Statuses are GpuStatus's (Ok, Unavailable, NotEnoughMemory, Failed); a status other than Ok raises
+``GpuError`` carrying it and ``sadcs_gpu_last_error()``. There is no CPU fallback: without the
+library, importing the bindings raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import enum
+from pathlib import Path
+
+import numpy as np
+
+_LIB_PATH = Path(__file__).resolve().parent / "lib" / "libsadcs_gpu.so"
+
+
+class GpuStatus(enum.IntEnum):
+    Ok = 0
+    Unavailable = 1
+    NotEnoughMemory = 2
+    Failed = 3
+
+
+class GpuError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        self.status = GpuStatus(status)
+        super().__init__(f"{self.status.name}: {message}")
+
+
+class Device(ctypes.Structure):
+    _fields_ = [("name", ctypes.c_char * 256), ("compute_major", ctypes.c_int32), ("compute_minor", ctypes.c_int32),
+                ("total_bytes", ctypes.c_int64), ("free_bytes", ctypes.c_int64)]
+
+
+class Stats(ctypes.Structure):
+    """GpuStats (gpusa.h:37-53)."""
+    _fields_ = [("device_bytes", ctypes.c_int64), ("ranking_bytes", ctypes.c_int64),
+                ("class_sort_bytes", ctypes.c_int64), ("merge_bytes", ctypes.c_int64),
+                ("pinned", ctypes.c_int32), ("character_passes", ctypes.c_int32),
+                ("doubling_rounds", ctypes.c_int32), ("reserved", ctypes.c_int32),
+                ("setup_seconds", ctypes.c_double), ("upload_seconds", ctypes.c_double),
+                ("device_seconds", ctypes.c_double), ("ranking_seconds", ctypes.c_double),
+                ("class_sort_seconds", ctypes.c_double), ("merge_seconds", ctypes.c_double),
+                ("bwt_seconds", ctypes.c_double), ("download_seconds", ctypes.c_double)]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_ if name != "reserved"}
+
+
+_u8p = ctypes.POINTER(ctypes.c_uint8)
+_u32p = ctypes.POINTER(ctypes.c_uint32)
+_i32p = ctypes.POINTER(ctypes.c_int32)
+_i64p = ctypes.POINTER(ctypes.c_int64)
+_ctxp = ctypes.c_void_p
+
+_lib = None
+
+
+def library_path() -> Path:
+    return _LIB_PATH
+
+
+def lib() -> ctypes.CDLL:
+    """The C ABI. Raises if libsadcs_gpu.so was not built: there is no fallback."""
+    global _lib
+    if _lib is None:
+        if not _LIB_PATH.exists():
+            raise ImportError(f"{_LIB_PATH} is missing: build it with `python -m sadcs_b200.build` "
+                              "(nvcc, sm_100a); there is no CPU fallback")
+        L = ctypes.CDLL(str(_LIB_PATH))
+        L.sadcs_gpu_memory_reserve.restype = ctypes.c_int64
+        L.sadcs_gpu_memory_reserve.argtypes = []
+        L.sadcs_gpu_sample_size.restype = ctypes.c_int64
+        L.sadcs_gpu_sample_size.argtypes = [ctypes.c_int64]
+        L.sadcs_gpu_query_device.restype = ctypes.c_int
+        L.sadcs_gpu_query_device.argtypes = [ctypes.POINTER(Device)]
+        L.sadcs_gpu_required_bytes.restype = ctypes.c_int64
+        L.sadcs_gpu_required_bytes.argtypes = [ctypes.c_int64]
+        L.sadcs_gpu_create_context.restype = ctypes.c_int
+        L.sadcs_gpu_create_context.argtypes = [ctypes.c_int64, ctypes.POINTER(_ctxp)]
+        L.sadcs_gpu_destroy_context.restype = None
+        L.sadcs_gpu_destroy_context.argtypes = [_ctxp]
+        L.sadcs_gpu_context_capacity.restype = ctypes.c_int64
+        L.sadcs_gpu_context_capacity.argtypes = [_ctxp]
+        L.sadcs_gpu_suffix_array.restype = ctypes.c_int
+        L.sadcs_gpu_suffix_array.argtypes = [_ctxp, _u8p, ctypes.c_int64, _i32p, ctypes.POINTER(Stats)]
+        L.sadcs_gpu_bwt.restype = ctypes.c_int
+        L.sadcs_gpu_bwt.argtypes = [_ctxp, _u8p, ctypes.c_int64, _u8p, _i32p, ctypes.POINTER(Stats)]
+        L.sadcs_gpu_rank_sample.restype = ctypes.c_int
+        L.sadcs_gpu_rank_sample.argtypes = [_u8p, ctypes.c_int64, _u32p, ctypes.POINTER(Stats)]
+        L.sadcs_gpu_allocate_pinned.restype = ctypes.c_void_p
+        L.sadcs_gpu_allocate_pinned.argtypes = [ctypes.c_size_t]
+        L.sadcs_gpu_free_pinned.restype = None
+        L.sadcs_gpu_free_pinned.argtypes = [ctypes.c_void_p]
+        L.sadcs_gpu_last_error.restype = ctypes.c_char_p
+        L.sadcs_gpu_last_error.argtypes = []
+        L.sadcs_gpu_build.restype = ctypes.c_int
+        L.sadcs_gpu_build.argtypes = [_ctxp, _u8p, ctypes.c_int64, _u32p, _u8p, _i64p, ctypes.POINTER(Stats)]
+        L.sadcs_gpu_build_device.restype = ctypes.c_int
+        L.sadcs_gpu_build_device.argtypes = [_ctxp, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p,
+                                             ctypes.c_void_p, _i64p, ctypes.c_void_p, ctypes.POINTER(Stats)]
+        L.sadcs_gpu_bwt_from_sa.restype = ctypes.c_int
+        L.sadcs_gpu_bwt_from_sa.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p,
+                                            _i64p, ctypes.c_void_p]
+        _lib = L
+    return _lib
+
+
+def last_error() -> str:
+    return lib().sadcs_gpu_last_error().decode(errors="replace")
+
+
+def _check(status: int) -> None:
+    if status != GpuStatus.Ok:
+        raise GpuError(status, last_error())
+
+
+def _as_text(text) -> np.ndarray:
+    if isinstance(text, (bytes, bytearray, memoryview)):
+        a = np.frombuffer(bytes(text), dtype=np.uint8)
+    else:
+        a = np.asarray(text)
+        if a.dtype != np.uint8:
+            raise TypeError(f"text must be uint8 bytes, got {a.dtype}")
+    return np.ascontiguousarray(a)
+
+
+def sample_size(n: int) -> int:
+    return int(lib().sadcs_gpu_sample_size(n))
+
+
+def memory_reserve() -> int:
+    return int(lib().sadcs_gpu_memory_reserve())
+
+
+def required_bytes(n: int) -> int:
+    return int(lib().sadcs_gpu_required_bytes(n))
+
+
+def query_device() -> dict:
+    d = Device()
+    _check(lib().sadcs_gpu_query_device(ctypes.byref(d)))
+    return {"name": d.name.decode(), "compute": (d.compute_major, d.compute_minor),
+            "total_bytes": d.total_bytes, "free_bytes": d.free_bytes}
+
+
+class Context:
+    """Device memory for texts of up to ``capacity`` bytes, reserved once (gpuCreateContext)."""
+
+    def __init__(self, capacity: int):
+        handle = _ctxp()
+        _check(lib().sadcs_gpu_create_context(int(capacity), ctypes.byref(handle)))
+        self._handle = handle
+
+    @property
+    def handle(self):
+        return self._handle
+
+    @property
+    def capacity(self) -> int:
+        return int(lib().sadcs_gpu_context_capacity(self._handle))
+
+    def close(self) -> None:
+        if getattr(self, "_handle", None):
+            lib().sadcs_gpu_destroy_context(self._handle)
+            self._handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _handle(context):
+    return context.handle if context is not None else None
+
+
+def suffix_array(text, context: Context | None = None, stats: Stats | None = None) -> np.ndarray:
+    """gpuSuffixArray: the int32 suffix array of text (n <= 2^31 - 1025)."""
+    t = _as_text(text)
+    n = len(t)
+    sa = np.empty(max(n, 1), np.int32)
+    _check(lib().sadcs_gpu_suffix_array(_handle(context), t.ctypes.data_as(_u8p), n, sa.ctypes.data_as(_i32p),
+                                        ctypes.byref(stats) if stats is not None else None))
+    return sa[:n]
+
+
+def bwt(text, context: Context | None = None, stats: Stats | None = None):
+    """gpuBwt: (BWT bytes, primary index) of text."""
+    t = _as_text(text)
+    n = len(t)
+    out = np.empty(max(n, 1), np.uint8)
+    primary = ctypes.c_int32(-1)
+    _check(lib().sadcs_gpu_bwt(_handle(context), t.ctypes.data_as(_u8p), n, out.ctypes.data_as(_u8p),
+                               ctypes.byref(primary), ctypes.byref(stats) if stats is not None else None))
+    return out[:n], int(primary.value)
+
+
+def rank_sample(text, stats: Stats | None = None) -> np.ndarray:
+    """gpuRankSample: ranks of the sample suffixes (cover mod 32), gpuSampleSize(n) entries."""
+    t = _as_text(text)
+    n = len(t)
+    ranks = np.empty(max(sample_size(n), 1), np.uint32)
+    _check(lib().sadcs_gpu_rank_sample(t.ctypes.data_as(_u8p), n, ranks.ctypes.data_as(_u32p),
+                                       ctypes.byref(stats) if stats is not None else None))
+    return ranks[:sample_size(n)]
+
+
+def build(text, want_sa: bool = True, want_bwt: bool = True, context: Context | None = None,
+          stats: Stats | None = None):
+    """SA (uint32) and/or BWT from one construction, host to host, n up to 2^32 - 256.
+
+    Returns (sa or None, bwt or None, primary or None)."""
+    t = _as_text(text)
+    n = len(t)
+    sa = np.empty(max(n, 1), np.uint32) if want_sa else None
+    out = np.empty(max(n, 1), np.uint8) if want_bwt else None
+    primary = ctypes.c_int64(-1)
+    _check(lib().sadcs_gpu_build(_handle(context), t.ctypes.data_as(_u8p), n,
+                                 sa.ctypes.data_as(_u32p) if sa is not None else None,
+                                 out.ctypes.data_as(_u8p) if out is not None else None, ctypes.byref(primary),
+                                 ctypes.byref(stats) if stats is not None else None))
+    return (sa[:n] if sa is not None else None, out[:n] if out is not None else None,
+            int(primary.value) if want_bwt else None)
+
+
+def build_device(d_text: int, n: int, d_sa: int | None, d_bwt: int | None, context: Context | None = None,
+                 stream: int | None = None, stats: Stats | None = None) -> int:
+    """Device-resident construction: raw device pointers (e.g. torch tensor data_ptr()), the caller's
+    stream handle (cudaStream_t as int, 0/None for the legacy default stream). Returns the primary
+    index (-1 when no BWT was asked for)."""
+    primary = ctypes.c_int64(-1)
+    _check(lib().sadcs_gpu_build_device(_handle(context), ctypes.c_void_p(d_text), int(n),
+                                        ctypes.c_void_p(d_sa) if d_sa else None,
+                                        ctypes.c_void_p(d_bwt) if d_bwt else None, ctypes.byref(primary),
+                                        ctypes.c_void_p(stream) if stream else None,
+                                        ctypes.byref(stats) if stats is not None else None))
+    return int(primary.value)
+
+
+def bwt_from_sa_device(d_text: int, n: int, d_sa: int, d_bwt: int, stream: int | None = None) -> int:
+    """The SA-to-BWT gather on device buffers; returns the primary index."""
+    primary = ctypes.c_int64(-1)
+    _check(lib().sadcs_gpu_bwt_from_sa(ctypes.c_void_p(d_text), int(n), ctypes.c_void_p(d_sa),
+                                       ctypes.c_void_p(d_bwt), ctypes.byref(primary),
+                                       ctypes.c_void_p(stream) if stream else None))
+    return int(primary.value)
+
+
+def allocate_pinned(nbytes: int) -> np.ndarray:
+    """Page-locked host memory as a uint8 array (freed with free_pinned)."""
+    ptr = lib().sadcs_gpu_allocate_pinned(int(nbytes))
+    if not ptr:
+        raise MemoryError("cannot allocate page-locked host memory")
+    buf = (ctypes.c_uint8 * max(int(nbytes), 1)).from_address(ptr)
+    arr = np.frombuffer(buf, dtype=np.uint8, count=int(nbytes))
+    return arr
+
+
+def free_pinned(array: np.ndarray) -> None:
+    lib().sadcs_gpu_free_pinned(ctypes.c_void_p(array.ctypes.data))

@@ -1,0 +1,139 @@
+// common.cuh - what every phase of the device construction shares.
+//
+// The difference cover modulo 32, D = {0, 1, 3, 8, 12, 19, 25} (the cover of the reference's GPU
+// path, src/common/differencecover.h:29-31 and src/cuda/devicecommon.cuh:31-36), with its lookup
+// tables generated at compile time from D and placed in __constant__ memory by static
+// initialisation, so every device that loads the module has them without an upload.
+//
+// Text layout in HBM: the text bytes, 8-byte aligned, followed by kTextPad zero bytes, so that a
+// 16-byte window at any position <= n + 31 stays inside the buffer and reads zeros past the end.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace sadcs {
+
+constexpr int kV = 32;        // cover period
+constexpr int kK = 7;         // cover size (sample positions per period)
+constexpr int kClasses = 7;   // distance to the next sample position: 0 (the sample) .. 6
+constexpr uint32_t kTextPad = 128;
+constexpr uint32_t kRankPad = 16;  // zero rank entries past the sample: a 7-rank window at any p <= n stays inside
+
+struct Cover {
+    uint8_t residue[kK];
+    uint8_t below[kV];           // cover residues below r
+    uint8_t classOf[kV];         // distance from residue r to the next cover residue
+    uint8_t tie[kV][kV];         // smallest k with a + k and b + k both sampled
+    uint8_t slot[kV][kV];        // [a][k]: index of sample a + k among the samples in [a, a + 32)
+};
+
+constexpr bool coverHas(int r) {
+    constexpr int d[kK] = {0, 1, 3, 8, 12, 19, 25};
+    for (int i = 0; i < kK; i++) {
+        if (d[i] == (r & (kV - 1))) return true;
+    }
+    return false;
+}
+
+constexpr Cover makeCover() {
+    Cover c{};
+    int k = 0;
+    for (int r = 0; r < kV; r++) {
+        if (coverHas(r)) c.residue[k++] = static_cast<uint8_t>(r);
+    }
+    for (int r = 0; r < kV; r++) {
+        int below = 0;
+        for (int q = 0; q < r; q++) below += coverHas(q) ? 1 : 0;
+        c.below[r] = static_cast<uint8_t>(below);
+        int d = 0;
+        while (!coverHas(r + d)) d++;
+        c.classOf[r] = static_cast<uint8_t>(d);
+    }
+    for (int a = 0; a < kV; a++) {
+        for (int b = 0; b < kV; b++) {
+            int t = 0;
+            while (!coverHas(a + t) || !coverHas(b + t)) t++;
+            c.tie[a][b] = static_cast<uint8_t>(t);
+        }
+        for (int t = 0; t < kV; t++) {
+            // samples in [a, a + t) = pack(a + t) - pack(a), with pack over absolute positions
+            int count = 0;
+            for (int q = a; q < a + t; q++) count += coverHas(q) ? 1 : 0;
+            c.slot[a][t] = static_cast<uint8_t>(count);
+        }
+    }
+    return c;
+}
+
+constexpr Cover kCoverTables = makeCover();
+static_assert(kCoverTables.classOf[2] == 1 && kCoverTables.classOf[26] == 6, "cover tables");
+
+__constant__ Cover cCover = makeCover();
+
+// Number of sample positions below p: a sample position's index in the compact rank array.
+inline uint64_t packHost(uint64_t p) {
+    return (p / kV) * kK + kCoverTables.below[p % kV];
+}
+
+__device__ __forceinline__ uint32_t pack(uint32_t p) {
+    return (p / kV) * kK + cCover.below[p % kV];
+}
+
+__device__ __forceinline__ uint32_t samplePosition(uint32_t t) {
+    return (t / kK) * kV + cCover.residue[t % kK];
+}
+
+inline uint64_t sampleSize(uint64_t n) {
+    return n == 0 ? 0 : packHost(n);
+}
+
+// Positions below n in class d.
+inline uint64_t classSize(uint64_t n, int d) {
+    uint64_t size = 0;
+    for (int r = 0; r < kV; r++) {
+        if (kCoverTables.classOf[r] == d) size += n / kV + (static_cast<uint64_t>(r) < n % kV ? 1 : 0);
+    }
+    return size;
+}
+
+__device__ __forceinline__ uint64_t byteSwap64(uint64_t x) {
+    const uint32_t lo = static_cast<uint32_t>(x), hi = static_cast<uint32_t>(x >> 32);
+    return (static_cast<uint64_t>(__byte_perm(lo, 0, 0x0123)) << 32) | __byte_perm(hi, 0, 0x0123);
+}
+
+// The 8 text bytes from p as a big-endian word (integer order = byte-string order); zeros past n.
+__device__ __forceinline__ uint64_t load8(const uint8_t* __restrict__ text, uint32_t p) {
+    const uint64_t* words = reinterpret_cast<const uint64_t*>(text);
+    const uint32_t w = p >> 3, shift = (p & 7) * 8;
+    const uint64_t lo = __ldg(words + w);
+    const uint64_t hi = __ldg(words + w + 1);
+    return byteSwap64(shift ? (lo >> shift) | (hi << (64 - shift)) : lo);
+}
+
+// 16 bytes from p as two big-endian words.
+__device__ __forceinline__ void load16(const uint8_t* __restrict__ text, uint32_t p, uint64_t& a, uint64_t& b) {
+    const uint64_t* words = reinterpret_cast<const uint64_t*>(text);
+    const uint32_t w = p >> 3, shift = (p & 7) * 8;
+    const uint64_t w0 = __ldg(words + w), w1 = __ldg(words + w + 1), w2 = __ldg(words + w + 2);
+    if (shift) {
+        a = byteSwap64((w0 >> shift) | (w1 << (64 - shift)));
+        b = byteSwap64((w1 >> shift) | (w2 << (64 - shift)));
+    } else {
+        a = byteSwap64(w0);
+        b = byteSwap64(w1);
+    }
+}
+
+__host__ __device__ __forceinline__ uint32_t ceilDiv(uint64_t a, uint64_t b) {
+    return static_cast<uint32_t>((a + b - 1) / b);
+}
+
+}  // namespace sadcs
+
+#define SADCS_TRY(call)                                 \
+    do {                                                \
+        const cudaError_t sadcsError_ = (call);         \
+        if (sadcsError_ != cudaSuccess) return sadcsError_; \
+    } while (0)

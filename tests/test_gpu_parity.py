@@ -1,0 +1,159 @@
+"""GPU construction vs. the oracle, bit for bit: the cases of the reference's runGpuCases
+(src/cli/selftest.cpp:543-606) and testGpuSampleRanks (:474-500), through the C ABI.
+
+The expected SA is the oracle's independent prefix-doubling construction (oracle/dcsa.c), itself
+pinned to the reference's own CPU output by tests/test_oracle.py; the expected BWT and sample ranks
+are derived from it in the reference's conventions (selftest.cpp:141-159, gpusa.h:65-73).
+"""
+import numpy as np
+import pytest
+
+import oracle
+import sadcs_b200 as sa
+from sadcs_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+LARGE = 1 << 22
+
+
+def _check(text, context=None, name=""):
+    text = np.asarray(text, dtype=np.uint8)
+    n = len(text)
+    expected = oracle.doubling_sa(text)
+    got = sa.suffix_array(text, context=context)
+    assert got.dtype == np.int32 and len(got) == n
+    mismatch = np.nonzero(got.astype(np.uint32) != expected)[0]
+    assert mismatch.size == 0, f"{name}: SA differs at {mismatch[:5]} (n={n})"
+    eb, ep = oracle.bwt_from_sa(text, expected)
+    # The BWT in place of a copy of the text, as `sadcs build --bwt --gpu` does it.
+    bwt, primary = sa.bwt(text, context=context)
+    assert primary == ep, f"{name}: primary {primary}, expected {ep}"
+    assert np.array_equal(bwt, eb), f"{name}: BWT differs at {np.nonzero(bwt != eb)[0][:5]}"
+    # Both from one construction.
+    s2, b2, p2 = sa.build(text, context=context)
+    assert np.array_equal(s2, expected) and np.array_equal(b2, eb) and p2 == ep, f"{name}: build() differs"
+
+
+def _check_ranks(text, name=""):
+    text = np.asarray(text, dtype=np.uint8)
+    expected = oracle.sample_ranks_from_sa(oracle.doubling_sa(text), len(text))
+    got = sa.rank_sample(text)
+    assert np.array_equal(got, expected), f"{name}: sample ranks differ at {np.nonzero(got != expected)[0][:5]}"
+
+
+WORDS = [b"", b"a", b"banana", b"mississippi", b"abracadabra", b"yabbadabbado"]
+
+
+@pytest.mark.parametrize("word", WORDS)
+def test_words(word):
+    _check(np.frombuffer(word, np.uint8), name=repr(word))
+
+
+def test_runs_and_binary_up_to_80():
+    rng = W.SplitMix(3)
+    for n in range(0, 81):
+        _check(W.run_text(n), name=f"run n={n}")
+        _check(W.random_text(rng, n, 2), name=f"sigma=2 n={n}")
+
+
+def test_sample_ranks_up_to_80():
+    rng = W.SplitMix(5)
+    for n in range(1, 81):
+        _check_ranks(W.run_text(n), name=f"run n={n}")
+        _check_ranks(W.random_text(rng, n, 2), name=f"sigma=2 n={n}")
+
+
+def test_structured():
+    rng = W.SplitMix(3)
+    _check(W.run_text(1000), name="run 1000")
+    _check(W.fibonacci_text(5000), name="fibonacci")
+    _check(W.fibonacci_text(5000, 0, 1), name="fibonacci 0/1")
+    _check(W.thue_morse_text(4096), name="thue-morse")
+    _check(np.zeros(1000, np.uint8), name="zeros")
+    run_b = W.run_text(2000)
+    run_b[-1] = ord("b")
+    _check(run_b, name="run then b")
+    b_run = W.run_text(2000)
+    b_run[0] = ord("b")
+    _check(b_run, name="b then run")
+    for period in (1, 2, 3, 5, 7, 31, 32, 33, 63, 64, 65, 1000):
+        _check(W.periodic_text(rng, 5000, period), name=f"period {period}")
+
+
+@pytest.mark.parametrize("sigma", [1, 2, 4, 26, 256])
+def test_random_alphabets(sigma):
+    rng = W.SplitMix(100 + sigma)
+    for i in range(10):
+        n = 1 + int(rng.below(20000)[0])
+        _check(W.random_text(rng, n, sigma), name=f"sigma={sigma} #{i}")
+
+
+def test_sample_ranks_structured():
+    rng = W.SplitMix(9)
+    for period in (1, 2, 3, 7, 31, 32, 33, 64, 65, 1000):
+        _check_ranks(W.periodic_text(rng, 5000, period), name=f"period {period}")
+    _check_ranks(np.frombuffer(b"banana", np.uint8), name="banana")
+    _check_ranks(W.fibonacci_text(5000, 0, 1), name="fibonacci 0/1")
+    _check_ranks(W.thue_morse_text(4096), name="thue-morse")
+    _check_ranks(W.random_text(rng, 5000, 256), name="sigma=256")
+
+
+@pytest.mark.parametrize("kind", ["run", "period33", "fibonacci", "thue-morse", "sigma4", "sigma256"])
+def test_large(kind):
+    rng = W.SplitMix(11)
+    text = {
+        "run": lambda: W.run_text(LARGE),
+        "period33": lambda: W.periodic_text(rng, LARGE, 33),
+        "fibonacci": lambda: W.fibonacci_text(LARGE),
+        "thue-morse": lambda: W.thue_morse_text(LARGE),
+        "sigma4": lambda: W.random_text(rng, LARGE, 4),
+        "sigma256": lambda: W.random_text(rng, LARGE, 256),
+    }[kind]()
+    _check(text, name=f"large {kind}")
+    _check_ranks(text, name=f"large {kind}")
+
+
+def test_context_reuse_and_refusal():
+    """selftest.cpp:505-541: one context, largest input first, empties, a refusal, then reuse."""
+    rng = W.SplitMix(3)
+    capacity = 20_000_000
+    with sa.Context(capacity) as ctx:
+        assert ctx.capacity == capacity
+        _check(W.random_text(rng, capacity, 4), context=ctx, name="context sigma=4 20M")
+        _check(W.random_text(rng, LARGE, 256), context=ctx, name="context sigma=256")
+        _check(np.frombuffer(b"banana", np.uint8), context=ctx, name="context banana")
+        _check(np.zeros(0, np.uint8), context=ctx, name="context empty")
+        _check(np.frombuffer(b"a", np.uint8), context=ctx, name="context a")
+        _check(W.fibonacci_text(LARGE), context=ctx, name="context fibonacci")
+        _check(W.periodic_text(rng, 5000, 33), context=ctx, name="context period 33")
+        for i in range(5):
+            _check(W.random_text(rng, 1 + int(rng.below(20000)[0]), 2), context=ctx, name=f"context sigma=2 #{i}")
+        with pytest.raises(sa.GpuError) as err:
+            sa.suffix_array(W.run_text(capacity + 1), context=ctx)
+        assert err.value.status == sa.GpuStatus.NotEnoughMemory
+        _check(W.random_text(rng, 5000, 26), context=ctx, name="context after refusal")
+
+
+def test_device_resident_and_gather():
+    """build_device on torch-owned HBM buffers, and the SA-to-BWT gather on its output."""
+    import torch
+
+    text = W.natural_text(1 << 20, seed=5)
+    n = len(text)
+    expected = oracle.doubling_sa(text)
+    eb, ep = oracle.bwt_from_sa(text, expected)
+    d_text = torch.from_numpy(text).cuda()
+    d_sa = torch.empty(n, dtype=torch.int32, device="cuda")
+    d_bwt = torch.empty(n, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    with sa.Context(n) as ctx:
+        primary = sa.build_device(d_text.data_ptr(), n, d_sa.data_ptr(), d_bwt.data_ptr(), context=ctx, stream=stream)
+    torch.cuda.synchronize()
+    assert primary == ep
+    assert np.array_equal(d_sa.cpu().numpy().view(np.uint32), expected)
+    assert np.array_equal(d_bwt.cpu().numpy(), eb)
+    d_bwt2 = torch.zeros(n, dtype=torch.uint8, device="cuda")
+    p2 = sa.bwt_from_sa_device(d_text.data_ptr(), n, d_sa.data_ptr(), d_bwt2.data_ptr(), stream=stream)
+    torch.cuda.synchronize()
+    assert p2 == ep and np.array_equal(d_bwt2.cpu().numpy(), eb)
