@@ -1,0 +1,448 @@
+"""bench.py - suffix array + BWT construction throughput on B200, and the reference CPU arm.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload natural256m|uniform8m|genome3g]
+    python bench.py --impl reference ...
+
+One step = one construction of the SA (uint32) and BWT of the workload's text, produced together.
+``value`` is device throughput with the text resident in HBM (CUDA events on the stream the library
+launches on, max over ranks); ``e2e`` is the same metric through the host C ABI (sadcs_gpu_build)
+from page-locked host memory, with the upload of the text and the download of SA and BWT inside
+the timed region. MB/s is MiB/s (the reference's convention, main.cpp:175-177).
+
+Roofline: HBM-bound integer work. ``roofline`` covers the dominant kernel (the final merge), timed
+live with CUDA events around its launch; its algorithmic bytes per input byte are 53 (class lists
+4, one 44-byte comparison record per element: 16 text bytes + 7 sample ranks, SA write 4, BWT write
+1). ``pipeline_roofline`` credits the whole construction with the fixed 82.125 bytes per input byte
+of the reference pipeline's named steps (sample ranking 12.375, class lists 11.75, merge 52, SA->BWT
+6). Peak = the measured HBM copy bandwidth in MEASURED_PEAKS.json (fallback 6650 GB/s).
+
+Multi-GPU: a single text does not shard, so N ranks build N independent replicas ("replicas",
+weak scaling); value = N * n / max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "input MB/s (bit-exact SA+BWT, % HBM roofline)"
+UNIT = "MiB/s"
+MIB = float(1 << 20)
+PIPELINE_BYTES_PER_INPUT_BYTE = 82.125
+MERGE_BYTES_PER_INPUT_BYTE = 53.0
+FALLBACK_HBM_GBS = 6650.0
+
+WORKLOADS = {
+    "natural256m": ("256 MiB natural-language-like text: 50k-word lowercase vocabulary (lengths 2-12), "
+                    "Zipf(1.1) words, '.\\n' every 10-30 words, 2% capitalised, seed 2",
+                    lambda W: W.natural_text(256 << 20, seed=2)),
+    "uniform8m": ("8 MiB i.i.d. uniform bytes, seed 1", lambda W: W.uniform_bytes(8 << 20, seed=1)),
+    "genome3g": ("3 GiB {A,C,G,T}: 2 GiB i.i.d. GC 0.41, then 1 GiB of mutated copies of 1 MiB segments "
+                 "(1% substitutions, 0.1% indels of 1-10), seed 3", lambda W: W.genome_text(3 << 30, seed=3)),
+}
+
+
+def hbm_peak():
+    path = ROOT / "MEASURED_PEAKS.json"
+    try:
+        return float(json.loads(path.read_text())["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+# ---- clocks -----------------------------------------------------------------------------------
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons for one GPU during the timed region."""
+
+    FIELDS = ["clocks.sm", "clocks.max.sm", "power.draw", "clocks_event_reasons.active",
+              "clocks_event_reasons.hw_slowdown", "clocks_event_reasons.hw_thermal_slowdown",
+              "clocks_event_reasons.sw_thermal_slowdown", "clocks_event_reasons.sw_power_cap"]
+
+    def __init__(self, uuid: str | None):
+        self.uuid = uuid
+        self.proc = None
+        self.lines: list[str] = []
+        self.thread = None
+
+    def start(self):
+        cmd = ["nvidia-smi", f"--query-gpu={','.join(self.FIELDS)}", "--format=csv,noheader,nounits", "-lms", "100"]
+        if self.uuid:
+            cmd += ["-i", self.uuid]
+        try:
+            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[4:8]):
+                if flag.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "samples": 0}
+        loaded = [v for v in sm if v >= 0.5 * max(sm)] or sm
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---- distributed plumbing -----------------------------------------------------------------------
+
+def dist_setup(gpus: int):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(value: float, world: int) -> float:
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(value: float, world: int) -> float:
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+# ---- CPU baseline (the reference's own CPU variant, or the oracle port) ----------------------------
+
+def cpu_baseline(text: np.ndarray, sample_bytes: int) -> dict:
+    import oracle
+
+    sample = np.ascontiguousarray(text[:sample_bytes])
+    if oracle.ref_available():
+        L = oracle.ref()
+        cores = oracle.host_cores()
+        L.ref_set_threads(cores)
+        t0 = time.perf_counter()
+        oracle.ref_sa(sample)
+        t1 = time.perf_counter()
+        oracle.ref_bwt(sample)
+        t2 = time.perf_counter()
+        return {"value": round(len(sample) / MIB / (t2 - t0), 3), "unit": UNIT, "cores": cores, "kind": "reference",
+                "sample": f"first {len(sample) / MIB:.0f} MiB of the workload text: reference CPU buildSuffixArray "
+                          f"({t1 - t0:.2f} s) then buildBwt ({t2 - t1:.2f} s), cover 128, {cores} threads"}
+    t0 = time.perf_counter()
+    sa = oracle.doubling_sa(sample)
+    oracle.bwt_from_sa(sample, sa)
+    t1 = time.perf_counter()
+    return {"value": round(len(sample) / MIB / (t1 - t0), 3), "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"first {len(sample) / MIB:.0f} MiB: oracle prefix-doubling SA + BWT, 1 thread"}
+
+
+def run_reference(args, world, rank) -> None:
+    """--impl reference: the reference's CPU implementation on this host's cores, rank 0 only."""
+    if rank != 0:
+        return
+    import oracle
+    from sadcs_b200 import workloads as W
+
+    desc, gen = WORKLOADS[args.workload]
+    text = gen(W)
+    n_sample = min(len(text), args.reference_sample_mib << 20)
+    sample = np.ascontiguousarray(text[:n_sample])
+    if oracle.ref_available():
+        L = oracle.ref()
+        cores = oracle.host_cores()
+        L.ref_set_threads(cores)
+        kind = "reference"
+
+        def step():
+            oracle.ref_sa(sample)
+            oracle.ref_bwt(sample)
+    else:
+        cores = 1
+        kind = "port"
+
+        def step():
+            sa = oracle.dc_sa(sample)
+            oracle.bwt_from_sa(sample, sa)
+    for _ in range(args.warmup):
+        step()
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        step()
+        times.append(time.perf_counter() - t0)
+    mean = sum(times) / len(times)
+    value = n_sample / MIB / mean
+    line = {"impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(mean * 1e3, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+            "config": {"workload": args.workload, "description": desc, "text_bytes": int(len(text)),
+                       "sample_bytes": int(n_sample), "outputs": "SA + BWT (two reference CPU runs)"},
+            "cpu_baseline": {"value": round(value, 3), "unit": UNIT, "cores": cores, "kind": kind,
+                             "sample": f"first {n_sample / MIB:.0f} MiB of the workload text per step, SA then BWT, "
+                                       f"{'reference CPU build (cover 128)' if kind == 'reference' else 'oracle port'}"},
+            "e2e": {"value": round(value, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---- our arm --------------------------------------------------------------------------------------
+
+def run_ours(args, world, rank, local) -> None:
+    import torch
+
+    import sadcs_b200 as sa
+    from sadcs_b200 import workloads as W
+
+    torch.cuda.set_device(local)
+    desc, gen = WORKLOADS[args.workload]
+    text = gen(W)
+    n = int(len(text))
+    props = torch.cuda.get_device_properties(local)
+    uuid = getattr(props, "uuid", None)
+    uuid = f"GPU-{uuid}" if uuid is not None and not str(uuid).startswith("GPU-") else (str(uuid) if uuid else None)
+
+    d_text = torch.from_numpy(text).to(f"cuda:{local}")
+    d_sa = torch.empty(n, dtype=torch.int32, device=f"cuda:{local}")
+    d_bwt = torch.empty(n, dtype=torch.uint8, device=f"cuda:{local}")
+    ctx = sa.Context(n)
+    stream = torch.cuda.current_stream()
+    handle = stream.cuda_stream
+    stats = sa.Stats()
+
+    def step():
+        return sa.build_device(d_text.data_ptr(), n, d_sa.data_ptr(), d_bwt.data_ptr(), context=ctx,
+                               stream=handle, stats=stats)
+
+    for _ in range(max(args.warmup, 0)):
+        step()
+    torch.cuda.synchronize()
+
+    sampler = ClockSampler(uuid)
+    sampler.start()
+    time.sleep(0.3)
+    barrier(world)
+    torch.cuda.synchronize()
+    start = torch.cuda.Event(enable_timing=True)
+    stop = torch.cuda.Event(enable_timing=True)
+    merge_ms, launches, phases = [], 0, {"ranking": [], "classes": [], "merge": []}
+    start.record(stream)
+    for _ in range(args.steps):
+        primary = step()
+        merge_ms.append(stats.merge_kernel_ms)
+        launches += int(stats.kernel_launches)
+        phases["ranking"].append(stats.ranking_device_ms)
+        phases["classes"].append(stats.class_sort_device_ms)
+        phases["merge"].append(stats.merge_device_ms)
+    stop.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    clocks = sampler.stop()
+    ms = start.elapsed_time(stop) / args.steps
+    ms_max = max_over_ranks(ms, world)
+    total_bytes = sum_over_ranks(float(n), world)
+    value = total_bytes / MIB / (ms_max / 1e3)
+
+    # Verification of the last step's output (size-independent checks on the device, test-side):
+    # SA is a permutation in suffix order by the Burkhardt-Karkkainen neighbour test, BWT = T[SA-1].
+    verified = verify_on_device(d_text, d_sa, d_bwt, primary) if args.verify else None
+
+    e2e = run_e2e(args, text, ctx, world) if args.e2e else None
+
+    if rank != 0:
+        return
+    peak, peak_kind = hbm_peak()
+    merge_avg = sum(merge_ms) / len(merge_ms)
+    merge_gbs = MERGE_BYTES_PER_INPUT_BYTE * n / (merge_avg / 1e3) / 1e9
+    pipe_gbs = PIPELINE_BYTES_PER_INPUT_BYTE * n / (ms / 1e3) / 1e9
+    roofline = {"bound": "hbm", "kernel": "mergeTiles<final> (level-0 tile merge writing SA + BWT)",
+                "achieved": round(merge_gbs, 1), "peak": peak, "unit": "GB/s", "frac": round(merge_gbs / peak, 4),
+                "traffic": None, "algorithmic_bytes_per_input_byte": MERGE_BYTES_PER_INPUT_BYTE,
+                "kernel_ms": round(merge_avg, 3), "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"}
+    traffic = profile_traffic(args.workload)
+    if traffic:
+        roofline["traffic"] = round(traffic * n)
+        roofline["traffic_source"] = "ncu dram__bytes_read.sum + dram__bytes_write.sum, per input byte, scaled"
+    line = {"metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms_max, 3), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+            "config": {"workload": args.workload, "description": desc, "text_bytes": n,
+                       "outputs": "SA (uint32) + BWT from one construction", "cover": "mod 32 (7 of 32)",
+                       "l2": "inputs larger than L2 (text %d MiB; working set %.1f GB)" % (
+                           n >> 20, sa.required_bytes(n) / 1e9),
+                       "parallelism": "replicas" if world > 1 else "single GPU"},
+            "roofline": roofline,
+            "pipeline_roofline": {"bound": "hbm", "achieved": round(pipe_gbs, 1), "peak": peak, "unit": "GB/s",
+                                  "frac": round(pipe_gbs / peak, 4),
+                                  "algorithmic_bytes_per_input_byte": PIPELINE_BYTES_PER_INPUT_BYTE},
+            "phases_ms": {k: round(sum(v) / len(v), 3) for k, v in phases.items()},
+            "character_passes": int(stats.character_passes), "doubling_rounds": int(stats.doubling_rounds),
+            "device_bytes_per_input_byte": round(stats.device_bytes / n, 3),
+            "clocks": clocks, "gpu_launches": launches, "verified": verified}
+    if e2e:
+        line["e2e"] = e2e
+    if world == 1 and args.cpu_sample_mib > 0:
+        line["cpu_baseline"] = cpu_baseline(text, args.cpu_sample_mib << 20)
+    print(json.dumps(line), flush=True)
+
+
+def run_e2e(args, text, ctx, world):
+    """sadcs_gpu_build from page-locked host memory: upload, construction, SA + BWT download."""
+    import ctypes
+
+    import sadcs_b200 as sa
+
+    n = len(text)
+    h_text = sa.allocate_pinned(n)
+    h_sa = sa.allocate_pinned(4 * n)
+    h_bwt = sa.allocate_pinned(n)
+    try:
+        h_text[:] = text
+        primary = ctypes.c_int64(-1)
+        L = sa.lib()
+
+        def step():
+            status = L.sadcs_gpu_build(ctx.handle, h_text.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)), n,
+                                       ctypes.cast(h_sa.ctypes.data, ctypes.POINTER(ctypes.c_uint32)),
+                                       h_bwt.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)), ctypes.byref(primary),
+                                       None)
+            if status != 0:
+                raise sa.GpuError(status, sa.last_error())
+
+        step()
+        steps = max(1, min(args.steps, args.e2e_steps))
+        barrier(world)
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            step()
+        seconds = (time.perf_counter() - t0) / steps
+        seconds = max_over_ranks(seconds, world)
+        total = sum_over_ranks(float(n), world)
+        return {"value": round(total / MIB / seconds, 3), "unit": UNIT, "h2d_bytes_per_step": n,
+                "d2h_bytes_per_step": 5 * n, "ms_per_step": round(seconds * 1e3, 3),
+                "api": "sadcs_gpu_build (host C ABI, page-locked buffers)", "steps": steps}
+    finally:
+        sa.free_pinned(h_text)
+        sa.free_pinned(h_sa)
+        sa.free_pinned(h_bwt)
+
+
+def verify_on_device(d_text, d_sa, d_bwt, primary) -> bool:
+    import torch
+
+    n = d_text.numel()
+    s = d_sa.to(torch.int64)
+    isa = torch.empty(n + 1, dtype=torch.int64, device=d_text.device)
+    isa[n] = -1
+    isa[s] = torch.arange(n, device=d_text.device)
+    if not bool((isa[:n][s] == torch.arange(n, device=d_text.device)).all()):
+        return False
+    t = d_text.to(torch.int64)
+    left, right = s[:-1], s[1:]
+    tl, tr = t[left], t[right]
+    nl, nr = isa[left + 1], isa[right + 1]
+    ok = (tl < tr) | ((tl == tr) & (nl < nr))
+    if not bool(ok.all()):
+        return False
+    rows = torch.arange(n, device=d_text.device)
+    row0 = int(rows[s == 0].item())
+    expected = torch.empty(n, dtype=torch.uint8, device=d_text.device)
+    expected[0] = d_text[n - 1]
+    keep = s != 0
+    idx = torch.where(rows < row0, rows + 1, rows)[keep]
+    expected[idx] = d_text[(s[keep] - 1)]
+    return bool(primary == row0 + 1 and torch.equal(expected, d_bwt))
+
+
+def profile_traffic(workload: str):
+    """DRAM bytes per input byte of the final merge kernel, from the committed ncu summary."""
+    path = ROOT / "profiles" / "traffic.json"
+    try:
+        data = json.loads(path.read_text())
+        return float(data[workload]["merge_dram_bytes_per_input_byte"])
+    except Exception:
+        return None
+
+
+def main() -> None:
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--workload", choices=sorted(WORKLOADS), default="natural256m")
+    p.add_argument("--cpu-sample-mib", type=int, default=64)
+    p.add_argument("--reference-sample-mib", type=int, default=64)
+    p.add_argument("--e2e-steps", type=int, default=3)
+    p.add_argument("--no-e2e", dest="e2e", action="store_false")
+    p.add_argument("--no-verify", dest="verify", action="store_false")
+    args = p.parse_args()
+    world, rank, local = dist_setup(args.gpus)
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank)
+        else:
+            run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

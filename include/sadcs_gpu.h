@@ -69,6 +69,12 @@ typedef struct sadcs_gpu_stats {
     double merge_seconds;
     double bwt_seconds;
     double download_seconds;
+    /* No counterpart: CUDA-event times on the construction's stream, and the kernels it launched. */
+    double ranking_device_ms;
+    double class_sort_device_ms;
+    double merge_device_ms;
+    double merge_kernel_ms;     /* the final merge kernel alone (the level that writes the SA/BWT) */
+    int64_t kernel_launches;
 } sadcs_gpu_stats;
 
 typedef struct sadcs_gpu_context sadcs_gpu_context;
@@ -133,6 +139,52 @@ int sadcs_gpu_build_device(sadcs_gpu_context* context, const uint8_t* d_text, in
  * convention above; *primary gets the sentinel's row. Device buffers, caller's stream. */
 int sadcs_gpu_bwt_from_sa(const uint8_t* d_text, int64_t n, const uint32_t* d_sa, uint8_t* d_bwt,
                           int64_t* primary, void* stream);
+
+/* No counterpart: peak device memory of a batch context for `texts` texts of `total` bytes together. */
+int64_t sadcs_gpu_required_bytes_batch(int64_t total, int64_t texts);
+
+/* No counterpart: a context for batches of up to max_texts texts of up to capacity bytes together. */
+int sadcs_gpu_create_batch_context(int64_t capacity, int64_t max_texts, sadcs_gpu_context** context);
+
+/* No counterpart: the SA (uint32, text-local positions) and/or BWT of `count` texts in ONE
+ * construction. texts: the texts back to back (text j at the sum of the lengths before it);
+ * outputs likewise back to back: text j's SA at sa + (sum of lengths before j), its BWT at the
+ * same offset in bwt; primaries[j] gets text j's primary index (0 for an empty text). Each text's
+ * SA and BWT are exactly what its own construction gives. */
+int sadcs_gpu_build_batch(sadcs_gpu_context* context, const uint8_t* texts, const int64_t* lengths, int64_t count,
+                          uint32_t* sa, uint8_t* bwt, int64_t* primaries, sadcs_gpu_stats* stats);
+
+/* No counterpart: the same with device-resident texts and outputs on the caller's stream (lengths
+ * and primaries are host arrays). */
+int sadcs_gpu_build_batch_device(sadcs_gpu_context* context, const uint8_t* d_texts, const int64_t* lengths,
+                                 int64_t count, uint32_t* d_sa, uint8_t* d_bwt, int64_t* primaries, void* stream,
+                                 sadcs_gpu_stats* stats);
+
+/* No counterpart: the reference checker's fast mode (src/common/checker.cpp:53-109) on the device.
+ * Device buffers: d_text (n bytes), d_sa (n uint32 entries). *bad_index gets -1 if the suffix array
+ * is correct, else the first failing SA index; *reason (if not NULL) a static description. Uses 4n
+ * bytes of temporary device memory. Returns SADCS_OK whenever the check ran. */
+int sadcs_gpu_check_suffix_array(const uint8_t* d_text, int64_t n, const uint32_t* d_sa, int64_t* bad_index,
+                                 const char** reason, void* stream);
+
+/* ---- serving (no counterpart) --------------------------------------------------------------------
+ * A request loop on the current device: requests are submitted at any time and complete
+ * asynchronously; queued small requests (up to small_limit bytes) are merged into one batched
+ * construction of up to batch_bytes / batch_texts; a construction starts when its planned peak fits
+ * memory_budget (<= 0: free memory minus the reserve) beside those running; `workers` threads with
+ * their own streams overlap their constructions on the device. Each result equals the result of the
+ * request's text built alone. text/sa/bwt stay owned by the caller until the request is waited for. */
+typedef struct sadcs_gpu_server sadcs_gpu_server;
+int sadcs_gpu_server_create(int64_t memory_budget, int32_t workers, int64_t small_limit, int64_t batch_bytes,
+                            int32_t batch_texts, sadcs_gpu_server** server);
+int sadcs_gpu_server_submit(sadcs_gpu_server* server, const uint8_t* text, int64_t n, uint32_t* sa, uint8_t* bwt,
+                            uint64_t* ticket);
+/* Blocks until the request is done (timeout_seconds < 0: no limit); latency gets queued, device and
+ * total seconds; batch_size the number of requests built together with it. */
+int sadcs_gpu_server_wait(sadcs_gpu_server* server, uint64_t ticket, double timeout_seconds, int64_t* primary,
+                          double* latency, int32_t* batch_size);
+void sadcs_gpu_server_counters(sadcs_gpu_server* server, int64_t* constructions, int64_t* launches);
+void sadcs_gpu_server_destroy(sadcs_gpu_server* server);
 
 /* No counterpart: the capacity (bytes of text) of a context. */
 int64_t sadcs_gpu_context_capacity(const sadcs_gpu_context* context);

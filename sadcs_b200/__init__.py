@@ -61,7 +61,10 @@ class Stats(ctypes.Structure):
                 ("setup_seconds", ctypes.c_double), ("upload_seconds", ctypes.c_double),
                 ("device_seconds", ctypes.c_double), ("ranking_seconds", ctypes.c_double),
                 ("class_sort_seconds", ctypes.c_double), ("merge_seconds", ctypes.c_double),
-                ("bwt_seconds", ctypes.c_double), ("download_seconds", ctypes.c_double)]
+                ("bwt_seconds", ctypes.c_double), ("download_seconds", ctypes.c_double),
+                ("ranking_device_ms", ctypes.c_double), ("class_sort_device_ms", ctypes.c_double),
+                ("merge_device_ms", ctypes.c_double), ("merge_kernel_ms", ctypes.c_double),
+                ("kernel_launches", ctypes.c_int64)]
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_ if name != "reserved"}
@@ -122,6 +125,32 @@ def lib() -> ctypes.CDLL:
         L.sadcs_gpu_bwt_from_sa.restype = ctypes.c_int
         L.sadcs_gpu_bwt_from_sa.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p,
                                             _i64p, ctypes.c_void_p]
+        L.sadcs_gpu_required_bytes_batch.restype = ctypes.c_int64
+        L.sadcs_gpu_required_bytes_batch.argtypes = [ctypes.c_int64, ctypes.c_int64]
+        L.sadcs_gpu_create_batch_context.restype = ctypes.c_int
+        L.sadcs_gpu_create_batch_context.argtypes = [ctypes.c_int64, ctypes.c_int64, ctypes.POINTER(_ctxp)]
+        L.sadcs_gpu_build_batch.restype = ctypes.c_int
+        L.sadcs_gpu_build_batch.argtypes = [_ctxp, _u8p, _i64p, ctypes.c_int64, _u32p, _u8p, _i64p,
+                                            ctypes.POINTER(Stats)]
+        L.sadcs_gpu_build_batch_device.restype = ctypes.c_int
+        L.sadcs_gpu_build_batch_device.argtypes = [_ctxp, ctypes.c_void_p, _i64p, ctypes.c_int64, ctypes.c_void_p,
+                                                   ctypes.c_void_p, _i64p, ctypes.c_void_p, ctypes.POINTER(Stats)]
+        L.sadcs_gpu_server_create.restype = ctypes.c_int
+        L.sadcs_gpu_server_create.argtypes = [ctypes.c_int64, ctypes.c_int32, ctypes.c_int64, ctypes.c_int64,
+                                              ctypes.c_int32, ctypes.POINTER(ctypes.c_void_p)]
+        L.sadcs_gpu_server_submit.restype = ctypes.c_int
+        L.sadcs_gpu_server_submit.argtypes = [ctypes.c_void_p, _u8p, ctypes.c_int64, _u32p, _u8p,
+                                              ctypes.POINTER(ctypes.c_uint64)]
+        L.sadcs_gpu_server_wait.restype = ctypes.c_int
+        L.sadcs_gpu_server_wait.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_double, _i64p,
+                                            ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int32)]
+        L.sadcs_gpu_server_counters.restype = None
+        L.sadcs_gpu_server_counters.argtypes = [ctypes.c_void_p, _i64p, _i64p]
+        L.sadcs_gpu_server_destroy.restype = None
+        L.sadcs_gpu_server_destroy.argtypes = [ctypes.c_void_p]
+        L.sadcs_gpu_check_suffix_array.restype = ctypes.c_int
+        L.sadcs_gpu_check_suffix_array.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, _i64p,
+                                                   ctypes.POINTER(ctypes.c_char_p), ctypes.c_void_p]
         _lib = L
     return _lib
 
@@ -165,11 +194,16 @@ def query_device() -> dict:
 
 
 class Context:
-    """Device memory for texts of up to ``capacity`` bytes, reserved once (gpuCreateContext)."""
+    """Device memory for texts of up to ``capacity`` bytes, reserved once (gpuCreateContext).
+    ``max_texts`` > 1 makes a batch context: batches of up to that many texts of ``capacity``
+    bytes together."""
 
-    def __init__(self, capacity: int):
+    def __init__(self, capacity: int, max_texts: int = 1):
         handle = _ctxp()
-        _check(lib().sadcs_gpu_create_context(int(capacity), ctypes.byref(handle)))
+        if max_texts == 1:
+            _check(lib().sadcs_gpu_create_context(int(capacity), ctypes.byref(handle)))
+        else:
+            _check(lib().sadcs_gpu_create_batch_context(int(capacity), int(max_texts), ctypes.byref(handle)))
         self._handle = handle
 
     @property
@@ -251,6 +285,49 @@ def build(text, want_sa: bool = True, want_bwt: bool = True, context: Context | 
             int(primary.value) if want_bwt else None)
 
 
+def required_bytes_batch(total: int, texts: int) -> int:
+    return int(lib().sadcs_gpu_required_bytes_batch(int(total), int(texts)))
+
+
+def build_batch(texts, want_sa: bool = True, want_bwt: bool = True, context: Context | None = None,
+                stats: Stats | None = None):
+    """SA and/or BWT of every text of a list in one construction (sadcs_gpu_build_batch).
+
+    Returns (list of SA arrays or None, list of BWT arrays or None, list of primaries or None)."""
+    arrays = [_as_text(t) for t in texts]
+    lengths = np.array([len(a) for a in arrays], dtype=np.int64)
+    packed = np.ascontiguousarray(np.concatenate(arrays) if arrays else np.zeros(0, np.uint8))
+    total = int(lengths.sum())
+    sa = np.empty(max(total, 1), np.uint32) if want_sa else None
+    out = np.empty(max(total, 1), np.uint8) if want_bwt else None
+    primaries = np.zeros(max(len(arrays), 1), np.int64)
+    _check(lib().sadcs_gpu_build_batch(_handle(context), packed.ctypes.data_as(_u8p) if packed.size else None,
+                                       lengths.ctypes.data_as(_i64p), len(arrays),
+                                       sa.ctypes.data_as(_u32p) if sa is not None else None,
+                                       out.ctypes.data_as(_u8p) if out is not None else None,
+                                       primaries.ctypes.data_as(_i64p),
+                                       ctypes.byref(stats) if stats is not None else None))
+    offsets = np.concatenate([[0], np.cumsum(lengths)])
+    sas = [sa[offsets[j]:offsets[j + 1]] for j in range(len(arrays))] if want_sa else None
+    bwts = [out[offsets[j]:offsets[j + 1]] for j in range(len(arrays))] if want_bwt else None
+    return sas, bwts, ([int(p) for p in primaries[:len(arrays)]] if want_bwt else None)
+
+
+def build_batch_device(d_texts: int, lengths, d_sa: int | None, d_bwt: int | None, context: Context | None = None,
+                       stream: int | None = None, stats: Stats | None = None):
+    """Device-resident batch: packed device texts, device outputs; returns the primaries."""
+    lengths = np.ascontiguousarray(np.asarray(lengths, dtype=np.int64))
+    primaries = np.zeros(max(len(lengths), 1), np.int64)
+    _check(lib().sadcs_gpu_build_batch_device(_handle(context), ctypes.c_void_p(d_texts),
+                                              lengths.ctypes.data_as(_i64p), len(lengths),
+                                              ctypes.c_void_p(d_sa) if d_sa else None,
+                                              ctypes.c_void_p(d_bwt) if d_bwt else None,
+                                              primaries.ctypes.data_as(_i64p),
+                                              ctypes.c_void_p(stream) if stream else None,
+                                              ctypes.byref(stats) if stats is not None else None))
+    return [int(p) for p in primaries[:len(lengths)]]
+
+
 def build_device(d_text: int, n: int, d_sa: int | None, d_bwt: int | None, context: Context | None = None,
                  stream: int | None = None, stats: Stats | None = None) -> int:
     """Device-resident construction: raw device pointers (e.g. torch tensor data_ptr()), the caller's
@@ -274,6 +351,16 @@ def bwt_from_sa_device(d_text: int, n: int, d_sa: int, d_bwt: int, stream: int |
     return int(primary.value)
 
 
+def check_suffix_array_device(d_text: int, n: int, d_sa: int, stream: int | None = None):
+    """The reference checker's fast mode on device buffers: (ok, first failing index, reason)."""
+    index = ctypes.c_int64(-1)
+    reason = ctypes.c_char_p()
+    _check(lib().sadcs_gpu_check_suffix_array(ctypes.c_void_p(d_text), int(n), ctypes.c_void_p(d_sa),
+                                              ctypes.byref(index), ctypes.byref(reason),
+                                              ctypes.c_void_p(stream) if stream else None))
+    return index.value < 0, int(index.value), reason.value.decode() if reason.value else None
+
+
 def allocate_pinned(nbytes: int) -> np.ndarray:
     """Page-locked host memory as a uint8 array (freed with free_pinned)."""
     ptr = lib().sadcs_gpu_allocate_pinned(int(nbytes))
@@ -286,3 +373,65 @@ def allocate_pinned(nbytes: int) -> np.ndarray:
 
 def free_pinned(array: np.ndarray) -> None:
     lib().sadcs_gpu_free_pinned(ctypes.c_void_p(array.ctypes.data))
+
+
+class Server:
+    """The request loop of the library (sadcs_gpu_server_*): submit texts at any time, wait for
+    their SA (uint32) and BWT. Queued small requests are built together in one batched
+    construction; constructions of different workers overlap on the device; admission is by
+    planned device footprint against ``memory_budget`` (<= 0: free memory minus the reserve)."""
+
+    def __init__(self, memory_budget: int = 0, workers: int = 2, small_limit: int = 4 << 20,
+                 batch_bytes: int = 256 << 20, batch_texts: int = 4096):
+        handle = ctypes.c_void_p()
+        _check(lib().sadcs_gpu_server_create(int(memory_budget), int(workers), int(small_limit), int(batch_bytes),
+                                             int(batch_texts), ctypes.byref(handle)))
+        self._handle = handle
+        self._pending = {}
+
+    def submit(self, text) -> int:
+        t = _as_text(text)
+        n = len(t)
+        sa = np.empty(max(n, 1), np.uint32)
+        out = np.empty(max(n, 1), np.uint8)
+        ticket = ctypes.c_uint64(0)
+        _check(lib().sadcs_gpu_server_submit(self._handle, t.ctypes.data_as(_u8p), n, sa.ctypes.data_as(_u32p),
+                                             out.ctypes.data_as(_u8p), ctypes.byref(ticket)))
+        self._pending[ticket.value] = (t, sa, out, n)
+        return int(ticket.value)
+
+    def wait(self, ticket: int, timeout: float = -1.0):
+        """Returns (sa, bwt, primary, latency (queued, device, total seconds), batch size)."""
+        primary = ctypes.c_int64(0)
+        latency = (ctypes.c_double * 3)()
+        batch = ctypes.c_int32(0)
+        status = lib().sadcs_gpu_server_wait(self._handle, int(ticket), float(timeout), ctypes.byref(primary),
+                                             latency, ctypes.byref(batch))
+        if status != GpuStatus.Ok and last_error() == "timed out":
+            raise TimeoutError(f"request {ticket} still running")
+        t, sa, out, n = self._pending.pop(ticket)
+        _check(status)
+        return sa[:n], out[:n], int(primary.value), tuple(latency), int(batch.value)
+
+    def counters(self):
+        c, l = ctypes.c_int64(0), ctypes.c_int64(0)
+        lib().sadcs_gpu_server_counters(self._handle, ctypes.byref(c), ctypes.byref(l))
+        return int(c.value), int(l.value)
+
+    def close(self) -> None:
+        if getattr(self, "_handle", None):
+            lib().sadcs_gpu_server_destroy(self._handle)
+            self._handle = None
+            self._pending.clear()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -20,7 +20,7 @@ __global__ void bwtGather(const uint8_t* __restrict__ text, const uint32_t* __re
     if (r == 0) bwt[0] = text[n - 1];
     if (r >= n) return;
     const uint32_t p = sa[r];
-    if (p != 0) bwt[r < row0 ? r + 1 : r] = text[p - 1];
+    if (p != 0 && p < n && row0 < n) bwt[r < row0 ? r + 1 : r] = text[p - 1];
 }
 
 inline cudaError_t bwtFromSa(const uint8_t* text, uint32_t n, const uint32_t* sa, uint8_t* bwt, uint32_t* row0Device,
@@ -30,10 +30,8 @@ inline cudaError_t bwtFromSa(const uint8_t* text, uint32_t n, const uint32_t* sa
         return cudaSuccess;
     }
     SADCS_TRY(cudaMemsetAsync(row0Device, 0, sizeof(uint32_t), stream));
-    bwtFindZero<<<(n + 255) / 256, 256, 0, stream>>>(sa, n, row0Device);
-    SADCS_TRY(cudaGetLastError());
-    bwtGather<<<(n + 255) / 256, 256, 0, stream>>>(text, sa, n, row0Device, bwt);
-    SADCS_TRY(cudaGetLastError());
+    SADCS_TRY(launch(bwtFindZero, (n + 255) / 256, 256, 0, stream, sa, n, row0Device));
+    SADCS_TRY(launch(bwtGather, (n + 255) / 256, 256, 0, stream, text, sa, n, row0Device, bwt));
     SADCS_TRY(cudaMemcpyAsync(hostWord, row0Device, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
     SADCS_TRY(cudaStreamSynchronize(stream));
     *row0 = *hostWord;

@@ -2,84 +2,210 @@
 //
 // Class d holds the positions whose next sample position is d characters ahead; class 0 is the
 // sample, ordered by its ranks. For i in class d >= 1, i + 1 is in class d - 1, so suffix i is
-// ordered by (T[i], suffix i + 1): class d is class d - 1 walked in order with n (the empty suffix,
-// smallest) in front, keeping the predecessors that fall in class d, stably sorted by their first
-// character. Position n - 1 comes from the prepended n and so leads its character bucket, as the
-// one-character suffix must.
+// ordered by (T[i], suffix i + 1): class d is class d - 1 walked in order with the text's end (the
+// empty suffix, smallest) in front, keeping the predecessors that fall in class d, stably sorted
+// by their first character. The text's last position comes from the prepended end and so leads its
+// character bucket, as the one-character suffix must.
 //
-// B200 shape: the walk, the filter, the character gather and the stable counting sort are one
-// radix pass (upsweep + scan + downsweep) through a filtering Loader, writing each class straight
-// into its slice of the concatenated lists.
+// Several texts: each global class list is the texts' class lists one after another (text order),
+// and each text is a segment of the pass: a segmented onesweep pass sorts all texts at once, every
+// text from its own digit bases. The walk, the filter, the character gather and the stable
+// counting sort are that one pass; the digit bases come from one streaming read of the text.
 #pragma once
+
+#include <algorithm>
 
 #include "common.cuh"
 #include "primitives.cuh"
 
 namespace sadcs {
 
-struct ClassLayout {
-    uint32_t start[kClasses + 1];
+// Device tables of the class phase for J texts (one text: J = 1), all in one block of words:
+//   rowBase[kClasses][J]                 first slot of (class, text) in the global lists
+//   elementStart[kClasses][J + 1]        segments of pass d: text j's class d - 1 plus its end
+//   tileStart[kClasses][J + 1]           the tiles of those segments
+struct ClassTables {
+    uint32_t texts = 0;
+    uint32_t* rowBase = nullptr;
+    uint32_t* elementStart = nullptr;
+    uint32_t* tileStart = nullptr;
+    static size_t words(uint32_t texts) { return static_cast<size_t>(kClasses) * (3 * texts + 2) + 16; }
+    void carve(uint32_t* base, uint32_t j) {
+        texts = j;
+        rowBase = base;
+        elementStart = rowBase + static_cast<size_t>(kClasses) * j;
+        tileStart = elementStart + static_cast<size_t>(kClasses) * (j + 1);
+    }
 };
 
-inline ClassLayout classLayout(uint64_t n) {
-    ClassLayout c{};
-    for (int d = 0; d < kClasses; d++) c.start[d + 1] = c.start[d] + static_cast<uint32_t>(classSize(n, d));
-    return c;
+// Host side of the class phase: sizes, offsets and tile counts from the text lengths.
+struct ClassPlan {
+    uint32_t start[kClasses + 1] = {};  // global class list offsets
+    uint32_t largest = 0;               // largest class over all texts together
+    uint32_t tiles[kClasses] = {};      // tiles of pass d (segmented)
+    uint32_t inputs[kClasses] = {};     // elements of pass d (class d - 1 plus one end per text)
+};
+
+// Fills the host copy of the tables (a host block laid out like ClassTables) and the plan.
+inline void planClasses(const uint64_t* lengths, uint32_t texts, uint32_t* tables, ClassPlan& plan) {
+    ClassTables t;
+    t.carve(tables, texts);
+    uint64_t total[kClasses] = {};
+    for (uint32_t j = 0; j < texts; j++) {
+        for (int d = 0; d < kClasses; d++) total[d] += classSize(lengths[j], d);
+    }
+    plan.start[0] = 0;
+    for (int d = 0; d < kClasses; d++) {
+        plan.start[d + 1] = plan.start[d] + static_cast<uint32_t>(total[d]);
+        plan.largest = std::max<uint32_t>(plan.largest, static_cast<uint32_t>(total[d]));
+    }
+    for (int d = 0; d < kClasses; d++) {
+        uint64_t offset = plan.start[d];
+        uint64_t elements = 0, tiles = 0;
+        for (uint32_t j = 0; j < texts; j++) {
+            t.rowBase[static_cast<size_t>(d) * texts + j] = static_cast<uint32_t>(offset);
+            offset += classSize(lengths[j], d);
+            const uint64_t input = d >= 1 ? classSize(lengths[j], d - 1) + 1 : 0;
+            t.elementStart[static_cast<size_t>(d) * (texts + 1) + j] = static_cast<uint32_t>(elements);
+            t.tileStart[static_cast<size_t>(d) * (texts + 1) + j] = static_cast<uint32_t>(tiles);
+            elements += input;
+            tiles += (input + kSortTile - 1) / kSortTile;
+        }
+        t.elementStart[static_cast<size_t>(d) * (texts + 1) + texts] = static_cast<uint32_t>(elements);
+        t.tileStart[static_cast<size_t>(d) * (texts + 1) + texts] = static_cast<uint32_t>(tiles);
+        plan.tiles[d] = static_cast<uint32_t>(tiles);
+        plan.inputs[d] = static_cast<uint32_t>(elements);
+    }
 }
 
-__global__ void classScatterSample(const uint32_t* __restrict__ ranks, uint32_t m, uint32_t* __restrict__ list) {
+inline size_t classScratchWords(uint64_t totalLength, uint32_t texts) {
+    // per-(class, text) histograms, then a radix scratch with room for every segmented tile
+    const uint64_t tiles = totalLength / kSortTile + static_cast<uint64_t>(texts) * 2 + 2;
+    return static_cast<size_t>(kClasses) * texts * 256 + 8 * 256 + 64 + static_cast<size_t>(tiles) * 256 + 64;
+}
+
+inline uint32_t* classRadixScratch(uint32_t* scratch, uint32_t texts) {
+    return scratch + static_cast<size_t>(kClasses) * texts * 256;
+}
+
+inline uint32_t* classErrorWord(uint32_t* scratch, uint32_t texts) {
+    return radixErrorWord(classRadixScratch(scratch, texts));
+}
+
+// Class 0: the live sample positions in rank order.
+__global__ void classScatterSample(const uint32_t* __restrict__ ranks, uint32_t slots, uint32_t live, TextSet texts,
+                                   uint32_t* __restrict__ list) {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t < m) list[ranks[t]] = samplePosition(t);
+    if (t >= slots) return;
+    const uint32_t p = samplePosition(t);
+    if (p >= texts.endOf(p)) return;  // past the end, or between texts
+    const uint32_t r = ranks[t];
+    if (r < live) list[r] = p;
 }
 
-// Element k of class d - 1 with n prepended; keeps p - 1 if it is in class d, keyed by T[p - 1].
+// Element k of text j's class d - 1 with the text's end prepended; keeps p - 1 if it is in class d
+// and in the text, keyed by T[p - 1].
 struct ClassLoader {
-    const uint32_t* __restrict__ previous;
+    const uint32_t* __restrict__ lists;       // global lists
+    const uint32_t* __restrict__ prevOffset;  // rowBase row of class d - 1: text j's slice offset
     const uint8_t* __restrict__ text;
-    uint32_t n;
+    TextSet texts;
     uint32_t d;
-    __device__ __forceinline__ bool pick(uint32_t k, uint32_t& q) const {
-        const uint32_t p = k == 0 ? n : previous[k - 1];
-        if (p == 0 || cCover.classOf[(p - 1) % kV] != d) return false;
-        q = p - 1;
-        return true;
-    }
-    __device__ __forceinline__ bool digit(uint32_t k, uint32_t& dig) const {
-        uint32_t q;
-        if (!pick(k, q)) return false;
-        dig = text[q];
-        return true;
-    }
-    __device__ __forceinline__ bool load(uint32_t k, uint8_t& key, uint32_t& v, uint32_t& dig) const {
-        uint32_t q;
-        if (!pick(k, q)) return false;
-        dig = text[q];
+    __device__ __forceinline__ bool load(uint32_t j, uint32_t, uint32_t k, uint8_t& key, uint32_t& v,
+                                         uint32_t& dig) const {
+        const uint32_t start = texts.startOf(j), end = texts.endOfText(j);
+        const uint32_t p = k == 0 ? end : lists[__ldg(prevOffset + j) + k - 1];
+        if (p <= start || p > end || cCover.classOf[(p - 1) % kV] != d) return false;
+        v = p - 1;
+        dig = text[v];
         key = static_cast<uint8_t>(dig);
-        v = q;
         return true;
     }
 };
 
 struct ClassStorer {
-    uint32_t* __restrict__ out;
-    __device__ __forceinline__ void store(uint32_t pos, uint8_t, uint32_t v) const { out[pos] = v; }
+    uint32_t* __restrict__ lists;
+    uint32_t lo, hi;  // class d's slots in the global lists
+    __device__ __forceinline__ void store(uint32_t, uint32_t pos, uint8_t, uint32_t v) const {
+        if (pos >= lo && pos < hi) lists[pos] = v;  // always, unless a look-back timed out
+    }
 };
 
-// Fills lists (n entries, laid out by classLayout(n)) from the sample ranks.
-inline cudaError_t sortClasses(const uint8_t* text, uint32_t n, const uint32_t* ranks, uint32_t* lists,
-                               uint32_t* scratch, cudaStream_t stream) {
-    const ClassLayout layout = classLayout(n);
-    const uint32_t m = layout.start[1];
-    if (m > 0) {
-        classScatterSample<<<(m + 255) / 256, 256, 0, stream>>>(ranks, m, lists);
-        SADCS_TRY(cudaGetLastError());
+// hist[(d * J + j) * 256 + c] = positions q of text j in class d with T[q] = c (zeroed by the caller).
+__global__ void __launch_bounds__(256) classHistogram(const uint8_t* __restrict__ text, uint32_t total,
+                                                      TextSet texts, uint32_t* __restrict__ hist) {
+    __shared__ uint32_t h[kClasses * 256];
+    const bool one = texts.count <= 1;
+    for (int i = threadIdx.x; i < kClasses * 256; i += blockDim.x) h[i] = 0;
+    __syncthreads();
+    const uint32_t lt = (1u << (threadIdx.x & 31)) - 1;
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x * 4;
+    for (uint64_t base = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) * 4; base < total;
+         base += stride) {
+        // four consecutive characters per thread, one 32-bit load (the text buffer is padded)
+        const uint32_t word = *reinterpret_cast<const uint32_t*>(text + base);
+        const uint32_t j = texts.textOf(static_cast<uint32_t>(base));
+        const uint32_t end = texts.endOfText(j);
+#pragma unroll
+        for (int b = 0; b < 4; b++) {
+            const uint64_t q = base + b;
+            const uint32_t c = (word >> (8 * b)) & 0xFF;
+            const uint32_t cls = q < end ? cCover.classOf[q % kV] : 0;
+            const uint32_t key = cls ? (cls * texts.count + j) * 256 + c : 0xFFFFFFFFu;
+            const uint32_t peers = __match_any_sync(0xffffffffu, key);
+            if (key != 0xFFFFFFFFu && (peers & lt) == 0) {
+                if (one) {
+                    atomicAdd(&h[key], static_cast<uint32_t>(__popc(peers)));
+                } else {
+                    atomicAdd(hist + key, static_cast<uint32_t>(__popc(peers)));
+                }
+            }
+        }
     }
+    if (one) {
+        __syncthreads();
+        for (int i = threadIdx.x; i < kClasses * 256; i += blockDim.x) {
+            if (h[i]) atomicAdd(hist + i, h[i]);
+        }
+    }
+}
+
+// Each 256-entry row r of hist becomes rowBase[r] + its exclusive prefix. One block per row.
+__global__ void __launch_bounds__(256) classDigitBase(uint32_t* __restrict__ hist, const uint32_t* __restrict__ rowBase) {
+    __shared__ uint32_t warpTotals[32];
+    uint32_t* row = hist + static_cast<size_t>(blockIdx.x) * 256;
+    const uint32_t v = row[threadIdx.x];
+    uint32_t total;
+    const uint32_t inclusive = blockInclusiveScan<OpSum>(v, warpTotals, total);
+    row[threadIdx.x] = rowBase[blockIdx.x] + inclusive - v;
+}
+
+// Fills lists (laid out by plan.start, text-major inside each class) from the sample ranks.
+// tables: the ClassTables block on the device; scratch: classScratchWords(total, J) words.
+// total: bytes of the concatenation (text buffer) scanned by the histogram.
+inline cudaError_t sortClasses(const uint8_t* text, uint32_t total, const TextSet& texts, const uint32_t* ranks,
+                               uint32_t slots, const ClassPlan& plan, const ClassTables& tables, uint32_t* lists,
+                               uint32_t* scratch, cudaStream_t stream) {
+    const uint32_t J = tables.texts;
+    const uint32_t live = plan.start[1];
+    if (live > 0) {
+        SADCS_TRY(launch(classScatterSample, (slots + 255) / 256, 256, 0, stream, ranks, slots, live, texts, lists));
+    }
+    uint32_t* hist = scratch;  // [kClasses][J][256]
+    const RadixScratch radix(classRadixScratch(scratch, J), 0);
+    SADCS_TRY(cudaMemsetAsync(hist, 0, static_cast<size_t>(kClasses) * J * 256 * 4, stream));
+    SADCS_TRY(cudaMemsetAsync(radix.control, 0, 8, stream));
+    const uint32_t blocks = std::min<uint32_t>(ceilDiv(total + 3ull, 256 * 4 * 8), 148 * 8);
+    SADCS_TRY(launch(classHistogram, blocks, 256, 0, stream, text, total, texts, hist));
+    SADCS_TRY(launch(classDigitBase, kClasses * J, 256, 0, stream, hist, tables.rowBase));
     for (int d = 1; d < kClasses; d++) {
-        if (layout.start[d + 1] == layout.start[d]) continue;
-        const uint32_t previousCount = layout.start[d] - layout.start[d - 1];
-        ClassLoader ld{lists + layout.start[d - 1], text, n, static_cast<uint32_t>(d)};
-        ClassStorer st{lists + layout.start[d]};
-        SADCS_TRY((radixPass<uint8_t>(ld, st, previousCount + 1, scratch, stream)));
+        if (plan.start[d + 1] == plan.start[d]) continue;
+        ClassLoader ld{lists, tables.rowBase + static_cast<size_t>(d - 1) * J, text, texts, static_cast<uint32_t>(d)};
+        ClassStorer st{lists, plan.start[d], plan.start[d + 1]};
+        ManySegments segs{tables.tileStart + static_cast<size_t>(d) * (J + 1),
+                          tables.elementStart + static_cast<size_t>(d) * (J + 1), J};
+        SADCS_TRY((radixOnesweepPass<uint8_t, ClassLoader, ClassStorer, ManySegments>(
+            ld, st, segs, plan.inputs[d], plan.tiles[d], hist + static_cast<size_t>(d) * J * 256, radix, stream)));
     }
     return cudaSuccess;
 }

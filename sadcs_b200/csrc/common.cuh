@@ -11,6 +11,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <utility>
 #include <cuda_runtime.h>
 
 namespace sadcs {
@@ -128,6 +129,37 @@ __device__ __forceinline__ void load16(const uint8_t* __restrict__ text, uint32_
 
 __host__ __device__ __forceinline__ uint32_t ceilDiv(uint64_t a, uint64_t b) {
     return static_cast<uint32_t>((a + b - 1) / b);
+}
+
+// The texts of one construction, concatenated in HBM. Text j occupies [start[j], end[j]), start[j]
+// a multiple of 32 so every position has the same residue modulo the cover period in its text and
+// in the concatenation; the bytes between texts are zero. blockText[p / 32] is the text whose range
+// contains or precedes block p / 32. With one text, blockText is null and its end is oneEnd.
+struct TextSet {
+    const uint32_t* blockText;
+    const uint32_t* start;
+    const uint32_t* end;
+    uint32_t count;
+    uint32_t oneEnd;
+    __device__ __forceinline__ uint32_t textOf(uint32_t p) const { return blockText ? __ldg(blockText + (p >> 5)) : 0; }
+    __device__ __forceinline__ uint32_t endOf(uint32_t p) const {
+        return blockText ? __ldg(end + __ldg(blockText + (p >> 5))) : oneEnd;
+    }
+    __device__ __forceinline__ uint32_t startOf(uint32_t text) const { return blockText ? __ldg(start + text) : 0; }
+    __device__ __forceinline__ uint32_t endOfText(uint32_t text) const { return blockText ? __ldg(end + text) : oneEnd; }
+};
+
+// Kernels launched by this thread since it last read the counter (reported in the stats).
+inline thread_local uint64_t tLaunches = 0;
+
+// Every kernel of the library is launched through here, so launches are counted.
+template <typename... Params, typename... Args>
+inline cudaError_t launch(void (*kernel)(Params...), dim3 grid, dim3 block, size_t shared, cudaStream_t stream,
+                          Args&&... args) {
+    if (grid.x == 0) return cudaSuccess;
+    kernel<<<grid, block, shared, stream>>>(std::forward<Args>(args)...);
+    ++tLaunches;
+    return cudaGetLastError();
 }
 
 }  // namespace sadcs

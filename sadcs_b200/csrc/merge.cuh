@@ -41,12 +41,17 @@ struct __align__(16) MergeRow {
     uint32_t c[kClasses];
 };
 
-struct __align__(16) MergeRecord {
-    uint64_t w0, w1;
+// w0, w1: the 16 text bytes at pos, big-endian; w2 is staging for the third aligned word while the
+// record is gathered (see gatherRecord). end: the end of pos's text (texts are ordered by it);
+// text: its index.
+struct __align__(8) MergeRecord {
+    uint64_t w0, w1, w2;
     uint32_t rank[kK];
     uint32_t pos;
+    uint32_t end;
+    uint32_t text;
 };
-static_assert(sizeof(MergeRecord) == 48, "record size");
+static_assert(sizeof(MergeRecord) == 64, "record size");
 
 struct MergeLevel {
     const uint32_t* lists;
@@ -56,13 +61,14 @@ struct MergeLevel {
 struct MergeArgs {
     const uint8_t* text;
     const uint32_t* ranks;
-    uint32_t n;
+    TextSet texts;
     MergeLevel level;
+    const uint32_t* outBase;  // per text: first output slot (SA entry / BWT byte)
+    uint32_t* rowZero;        // per text: the output row of the text's first suffix
     const MergeRow* rowsIn;  // null: one tile over the whole level
     MergeRow* rowsOut;       // levels >= 1
-    uint32_t* sa;            // level 0, optional
-    uint8_t* bwt;            // level 0, optional: the final n-byte BWT
-    uint32_t row0;           // output row of suffix 0
+    uint32_t* sa;            // level 0, optional: text-local positions
+    uint8_t* bwt;            // level 0, optional: the final BWT bytes of every text
     uint32_t* error;         // set nonzero if a window set exceeds the capacity (never, by construction)
 };
 
@@ -71,18 +77,29 @@ __device__ __forceinline__ uint64_t prefixMask(uint32_t c) {
 }
 
 __device__ __forceinline__ void loadRecord(const uint8_t* __restrict__ text, const uint32_t* __restrict__ ranks,
-                                           uint32_t p, MergeRecord& r) {
+                                           const TextSet& texts, uint32_t p, MergeRecord& r) {
     load16(text, p, r.w0, r.w1);
     const uint32_t base = pack(p);
 #pragma unroll
     for (int s = 0; s < kK; s++) r.rank[s] = __ldg(ranks + base + s);
     r.pos = p;
+    r.text = texts.textOf(p);
+    r.end = texts.endOfText(r.text);
 }
 
+// Cover tables the comparison reads, in shared memory: the threads of a warp index them at
+// different places, which constant memory would serialise.
+struct MergeTables {
+    uint8_t tie[kV][kV];
+    uint8_t slot[kV][kV];
+};
+
 __device__ __forceinline__ bool lessRecord(const MergeRecord& a, const MergeRecord& b,
-                                           const uint8_t* __restrict__ text, uint32_t n) {
+                                           const uint8_t* __restrict__ text, const MergeTables& tb) {
+    if (a.end != b.end) return a.end < b.end;  // different texts: text order
+    const uint32_t n = a.end;
     const uint32_t i = a.pos, j = b.pos;
-    const uint32_t k = cCover.tie[i % kV][j % kV];
+    const uint32_t k = tb.tie[i % kV][j % kV];
     const uint32_t common = min(k, min(n - i, n - j));
     uint64_t x = a.w0, y = b.w0;
     if (common < 8) {
@@ -112,7 +129,45 @@ __device__ __forceinline__ bool lessRecord(const MergeRecord& a, const MergeReco
         }
     }
     if (common < k || i + k == n || j + k == n) return i > j;  // one is a prefix of the other
-    return a.rank[cCover.slot[i % kV][k]] < b.rank[cCover.slot[j % kV][k]];
+    return a.rank[tb.slot[i % kV][k]] < b.rank[tb.slot[j % kV][k]];
+}
+
+__device__ __forceinline__ void cpAsync8(void* sharedDst, const void* globalSrc) {
+    const uint32_t dst = static_cast<uint32_t>(__cvta_generic_to_shared(sharedDst));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(globalSrc) : "memory");
+}
+
+__device__ __forceinline__ void cpAsync4(void* sharedDst, const void* globalSrc) {
+    const uint32_t dst = static_cast<uint32_t>(__cvta_generic_to_shared(sharedDst));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(dst), "l"(globalSrc) : "memory");
+}
+
+__device__ __forceinline__ void cpAsyncWaitAll() {
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
+
+// Issues the gather of r's raw text words (the three aligned words covering [p, p + 16)) and its
+// 7 sample ranks as asynchronous copies into shared memory: every load of every record of the
+// thread is in flight at once. finishRecord() turns the raw words into big-endian windows.
+__device__ __forceinline__ void gatherRecord(const uint8_t* __restrict__ text, const uint32_t* __restrict__ ranks,
+                                             const TextSet& texts, uint32_t p, MergeRecord& r) {
+    const uint64_t* words = reinterpret_cast<const uint64_t*>(text) + (p >> 3);
+    cpAsync8(&r.w0, words);
+    cpAsync8(&r.w1, words + 1);
+    cpAsync8(&r.w2, words + 2);
+    const uint32_t* rk = ranks + pack(p);
+#pragma unroll
+    for (int s = 0; s < kK; s++) cpAsync4(&r.rank[s], rk + s);
+    r.pos = p;
+    r.text = texts.textOf(p);
+    r.end = texts.endOfText(r.text);
+}
+
+__device__ __forceinline__ void finishRecord(MergeRecord& r) {
+    const uint32_t shift = (r.pos & 7) * 8;
+    const uint64_t a = r.w0, b = r.w1, c = r.w2;
+    r.w0 = byteSwap64(shift ? (a >> shift) | (b << (64 - shift)) : a);
+    r.w1 = byteSwap64(shift ? (b >> shift) | (c << (64 - shift)) : b);
 }
 
 struct MergeTileInfo {
@@ -141,6 +196,15 @@ __global__ void __launch_bounds__(kMergeThreads) mergeTiles(MergeArgs a) {
     uint16_t* cnt = reinterpret_cast<uint16_t*>(rec + kMergeCap);
     uint32_t* lr = reinterpret_cast<uint32_t*>(cnt + kMergeCap * 8);
     __shared__ MergeTileInfo t;
+    __shared__ __align__(16) MergeTables tb;
+    {
+        const uint32_t* src = reinterpret_cast<const uint32_t*>(&cCover.tie[0][0]);
+        uint32_t* dst = reinterpret_cast<uint32_t*>(&tb.tie[0][0]);
+        for (int i = threadIdx.x; i < kV * kV / 4; i += kMergeThreads) dst[i] = src[i];
+        const uint32_t* src2 = reinterpret_cast<const uint32_t*>(&cCover.slot[0][0]);
+        uint32_t* dst2 = reinterpret_cast<uint32_t*>(&tb.slot[0][0]);
+        for (int i = threadIdx.x; i < kV * kV / 4; i += kMergeThreads) dst2[i] = src2[i];
+    }
 
     if (threadIdx.x == 0) {
         const uint32_t* st = a.level.start;
@@ -211,13 +275,36 @@ __global__ void __launch_bounds__(kMergeThreads) mergeTiles(MergeArgs a) {
 
     const uint32_t size = t.size;
     const uint32_t* st = a.level.start;
-    for (uint32_t e = threadIdx.x; e < size; e += kMergeThreads) {
-        const int l = listOfElement(t.seg, e);
-        const uint32_t p = a.level.lists[st[l] + t.win[l] + (e - t.seg[l])];
-        loadRecord(a.text, a.ranks, p, rec[e]);
+    // Positions first (list reads, coalesced), then every record's gather in flight at once.
+    constexpr int kItems = (kMergeCap + kMergeThreads - 1) / kMergeThreads;
+    uint32_t pos[kItems];
+#pragma unroll
+    for (int j = 0; j < kItems; j++) {
+        const uint32_t e = threadIdx.x + j * kMergeThreads;
+        pos[j] = 0;
+        if (e < size) {
+            const int l = listOfElement(t.seg, e);
+            uint32_t p = a.level.lists[st[l] + t.win[l] + (e - t.seg[l])];
+            if (p >= a.texts.endOf(p)) {  // cannot happen for valid class lists; never read out of range
+                atomicExch(a.error, 3u);
+                p = 0;
+            }
+            pos[j] = p;
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < kItems; j++) {
+        const uint32_t e = threadIdx.x + j * kMergeThreads;
+        if (e < size) gatherRecord(a.text, a.ranks, a.texts, pos[j], rec[e]);
     }
     uint32_t* cnt32 = reinterpret_cast<uint32_t*>(cnt);
     for (uint32_t i = threadIdx.x; i < size * 4; i += kMergeThreads) cnt32[i] = 0;
+    cpAsyncWaitAll();
+#pragma unroll
+    for (int j = 0; j < kItems; j++) {
+        const uint32_t e = threadIdx.x + j * kMergeThreads;
+        if (e < size) finishRecord(rec[e]);
+    }
     __syncthreads();
 
     const uint32_t items = t.pairStart[kPairs], c = t.chunk;
@@ -232,7 +319,7 @@ __global__ void __launch_bounds__(kMergeThreads) mergeTiles(MergeArgs a) {
         uint32_t lo = d > lenB ? d - lenB : 0, hi = min(d, lenA);
         while (lo < hi) {
             const uint32_t mid = (lo + hi) >> 1;
-            if (lessRecord(rec[sa + mid], rec[sb + d - 1 - mid], a.text, a.n)) {
+            if (lessRecord(rec[sa + mid], rec[sb + d - 1 - mid], a.text, tb)) {
                 lo = mid + 1;
             } else {
                 hi = mid;
@@ -240,7 +327,7 @@ __global__ void __launch_bounds__(kMergeThreads) mergeTiles(MergeArgs a) {
         }
         uint32_t i = lo, j = d - lo;
         for (; d < end; d++) {
-            if (j == lenB || (i < lenA && lessRecord(rec[sa + i], rec[sb + j], a.text, a.n))) {
+            if (j == lenB || (i < lenA && lessRecord(rec[sa + i], rec[sb + j], a.text, tb))) {
                 cnt[(sa + i) * 8 + lb] = static_cast<uint16_t>(j);
                 i++;
             } else {
@@ -274,9 +361,13 @@ __global__ void __launch_bounds__(kMergeThreads) mergeTiles(MergeArgs a) {
             continue;
         }
         if constexpr (kFinal) {
-            const uint32_t p = rec[e].pos;
-            if (a.sa) a.sa[g] = p;
-            if (a.bwt && p != 0) a.bwt[g < a.row0 ? g + 1 : g] = a.text[p - 1];
+            const uint32_t p = rec[e].pos, tj = rec[e].text;
+            const uint32_t first = a.texts.startOf(tj);
+            if (a.sa) a.sa[g] = p - first;
+            if (a.bwt && p != first) {
+                const uint32_t base = __ldg(a.outBase + tj), row = g - base, zero = __ldg(a.rowZero + tj);
+                a.bwt[base + (row < zero ? row + 1 : row)] = a.text[p - 1];
+            }
         } else {
             if (g % kMergeR == 0) {
                 const int l = listOfElement(t.seg, e);
@@ -311,29 +402,44 @@ __global__ void mergeWriteSentinel(MergeRow* row, MergeLevel level) {
     }
 }
 
-// out += number of elements of list threadIdx.x smaller than suffix 0: its output row.
-__global__ void mergeSuffixZeroRow(MergeArgs a, uint32_t* out) {
+// rowZero[j] += the elements of list threadIdx.x in text j smaller than text j's first suffix: its
+// output row within the text. One block per text. rowBase: the class tables' first slot of every
+// (class, text); classEnd: plan.start[1..7].
+__global__ void mergeSuffixZeroRows(MergeArgs a, const uint32_t* __restrict__ rowBase, MergeLevel classes,
+                                    uint32_t* rowZero) {
+    __shared__ MergeTables tb;
+    for (int i = threadIdx.x; i < kV * kV; i += blockDim.x) {
+        (&tb.tie[0][0])[i] = (&cCover.tie[0][0])[i];
+        (&tb.slot[0][0])[i] = (&cCover.slot[0][0])[i];
+    }
+    __syncthreads();
     const int b = threadIdx.x;
+    const uint32_t j = blockIdx.x, J = a.texts.count;
     if (b >= kClasses) return;
     MergeRecord zero;
-    loadRecord(a.text, a.ranks, 0, zero);
-    const uint32_t* list = a.level.lists + a.level.start[b];
-    uint32_t lo = 0, hi = a.level.start[b + 1] - a.level.start[b];
+    loadRecord(a.text, a.ranks, a.texts, a.texts.startOf(j), zero);
+    const uint32_t first = rowBase[static_cast<size_t>(b) * J + j];
+    const uint32_t last = j + 1 < J ? rowBase[static_cast<size_t>(b) * J + j + 1] : classes.start[b + 1];
+    const uint32_t* list = a.level.lists + first;
+    uint32_t lo = 0, hi = last - first;
     while (lo < hi) {
         const uint32_t mid = (lo + hi) >> 1;
         MergeRecord r;
-        loadRecord(a.text, a.ranks, list[mid], r);
-        if (lessRecord(r, zero, a.text, a.n)) {
+        loadRecord(a.text, a.ranks, a.texts, list[mid], r);
+        if (lessRecord(r, zero, a.text, tb)) {
             lo = mid + 1;
         } else {
             hi = mid;
         }
     }
-    atomicAdd(out, lo);
+    atomicAdd(rowZero + j, lo);
 }
 
-__global__ void mergeBwtHead(const uint8_t* __restrict__ text, uint32_t n, uint8_t* bwt) {
-    if (threadIdx.x == 0 && n > 0) bwt[0] = text[n - 1];
+// bwt[outBase[j]] = the last character of text j (the sentinel's row).
+__global__ void mergeBwtHeads(const uint8_t* __restrict__ text, TextSet texts, const uint32_t* __restrict__ outBase,
+                              uint8_t* bwt) {
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j < texts.count) bwt[outBase[j]] = text[texts.endOfText(j) - 1];
 }
 
 // Sizes of every level, planned on the host from n alone.
@@ -370,21 +476,23 @@ inline MergePlan planMerge(const uint32_t* classStart) {
     return p;
 }
 
-// Merges the class lists of text into sa and/or bwt (either may be null). splitters and rows are
-// scratch sized by planMerge; counter is one device word (scratch).
-inline cudaError_t mergeClasses(const uint8_t* text, const uint32_t* ranks, uint32_t n, const uint32_t* lists,
-                                const MergePlan& plan, uint32_t* splitters, MergeRow* rows, uint32_t* sa,
-                                uint8_t* bwt, uint32_t* counter, uint32_t* hostWord, cudaStream_t stream,
-                                uint32_t* row0Out) {
-    static uint64_t configured[2] = {0, 0};
+// Merges the class lists of the texts into sa and/or bwt (either may be null). splitters and rows
+// are scratch sized by planMerge; counter is one device word (scratch); rowZero and outBase are per
+// text (rowZero is filled here when a BWT is asked for); rowBase: the class tables' row bases.
+inline cudaError_t mergeClasses(const uint8_t* text, const uint32_t* ranks, const TextSet& texts, const uint32_t* lists,
+                                const MergePlan& plan, const uint32_t* rowBase, const uint32_t* outBase,
+                                uint32_t* rowZero, uint32_t* splitters, MergeRow* rows, uint32_t* sa, uint8_t* bwt,
+                                uint32_t* counter, uint32_t* hostWord, cudaStream_t stream,
+                                cudaEvent_t finalStart = nullptr, cudaEvent_t finalStop = nullptr) {
+    static uint64_t configured = 0;
     int device = 0;
     SADCS_TRY(cudaGetDevice(&device));
-    if (!(configured[0] >> (device & 63) & 1)) {
+    if (!(configured >> (device & 63) & 1)) {
         SADCS_TRY(cudaFuncSetAttribute(mergeTiles<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(mergeSharedBytes())));
         SADCS_TRY(cudaFuncSetAttribute(mergeTiles<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(mergeSharedBytes())));
-        configured[0] |= uint64_t(1) << (device & 63);
+        configured |= uint64_t(1) << (device & 63);
     }
     MergeLevel level[kMaxLevels];
     for (int L = 0; L <= plan.top; L++) {
@@ -393,29 +501,24 @@ inline cudaError_t mergeClasses(const uint8_t* text, const uint32_t* ranks, uint
     }
     for (int L = 1; L <= plan.top; L++) {
         const uint32_t count = plan.start[L][kClasses];
-        mergeGatherSplitters<<<(count + 255) / 256, 256, 0, stream>>>(level[L - 1].lists, level[L - 1], level[L],
-                                                                      const_cast<uint32_t*>(level[L].lists));
-        SADCS_TRY(cudaGetLastError());
+        SADCS_TRY(launch(mergeGatherSplitters, (count + 255) / 256, 256, 0, stream, level[L - 1].lists, level[L - 1],
+                         level[L], const_cast<uint32_t*>(level[L].lists)));
     }
-    SADCS_TRY(cudaMemsetAsync(counter, 0, 2 * sizeof(uint32_t), stream));  // [0] suffix 0's row, [1] error
+    SADCS_TRY(cudaMemsetAsync(counter, 0, sizeof(uint32_t), stream));  // error word
     MergeArgs base{};
     base.text = text;
     base.ranks = ranks;
-    base.n = n;
-    base.error = counter + 1;
-    uint32_t row0 = 0;
-    if (bwt && n > 0) {
+    base.texts = texts;
+    base.outBase = outBase;
+    base.rowZero = rowZero;
+    base.error = counter;
+    if (bwt) {
         MergeArgs z = base;
         z.level = level[0];
-        mergeSuffixZeroRow<<<1, 32, 0, stream>>>(z, counter);
-        SADCS_TRY(cudaGetLastError());
-        SADCS_TRY(cudaMemcpyAsync(hostWord, counter, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
-        SADCS_TRY(cudaStreamSynchronize(stream));
-        row0 = *hostWord;
-        mergeBwtHead<<<1, 32, 0, stream>>>(text, n, bwt);
-        SADCS_TRY(cudaGetLastError());
+        SADCS_TRY(cudaMemsetAsync(rowZero, 0, sizeof(uint32_t) * texts.count, stream));
+        SADCS_TRY(launch(mergeSuffixZeroRows, texts.count, 32, 0, stream, z, rowBase, level[0], rowZero));
+        SADCS_TRY(launch(mergeBwtHeads, (texts.count + 255) / 256, 256, 0, stream, text, texts, outBase, bwt));
     }
-    if (row0Out) *row0Out = row0;
     for (int L = plan.top; L >= 0; L--) {
         MergeArgs args = base;
         args.level = level[L];
@@ -424,16 +527,17 @@ inline cudaError_t mergeClasses(const uint8_t* text, const uint32_t* ranks, uint
         if (L == 0) {
             args.sa = sa;
             args.bwt = bwt;
-            args.row0 = row0;
-            mergeTiles<true><<<tiles, kMergeThreads, mergeSharedBytes(), stream>>>(args);
+            if (finalStart) SADCS_TRY(cudaEventRecord(finalStart, stream));
+            SADCS_TRY(launch(mergeTiles<true>, tiles, kMergeThreads, mergeSharedBytes(), stream, args));
+            if (finalStop) SADCS_TRY(cudaEventRecord(finalStop, stream));
         } else {
             args.rowsOut = rows + plan.rowIndex[L - 1];
-            mergeWriteSentinel<<<1, 32, 0, stream>>>(rows + plan.rowIndex[L - 1] + plan.tiles[L - 1], level[L]);
-            mergeTiles<false><<<tiles, kMergeThreads, mergeSharedBytes(), stream>>>(args);
+            SADCS_TRY(launch(mergeWriteSentinel, 1, 32, 0, stream, rows + plan.rowIndex[L - 1] + plan.tiles[L - 1],
+                             level[L]));
+            SADCS_TRY(launch(mergeTiles<false>, tiles, kMergeThreads, mergeSharedBytes(), stream, args));
         }
-        SADCS_TRY(cudaGetLastError());
     }
-    SADCS_TRY(cudaMemcpyAsync(hostWord, counter + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+    SADCS_TRY(cudaMemcpyAsync(hostWord, counter, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
     SADCS_TRY(cudaStreamSynchronize(stream));
     return *hostWord ? cudaErrorUnknown : cudaSuccess;
 }

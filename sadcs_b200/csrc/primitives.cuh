@@ -13,6 +13,8 @@
 // sorts and the filtered class passes.
 #pragma once
 
+#include <algorithm>
+
 #include "common.cuh"
 
 namespace sadcs {
@@ -144,59 +146,88 @@ cudaError_t deviceScan(const uint32_t* in, uint32_t* out, uint32_t count, uint32
     }
     const uint32_t blocks = ceilDiv(count, kScanTile);
     if (blocks == 1) {
-        scanDownKernel<Op, kInclusive><<<1, kScanThreads, 0, stream>>>(in, out, count, nullptr, totalOut);
+        SADCS_TRY(launch(scanDownKernel<Op, kInclusive>, 1, kScanThreads, 0, stream, in, out, count, nullptr, totalOut));
         return cudaGetLastError();
     }
     uint32_t* partials = scratch;
-    scanReduceKernel<Op><<<blocks, kScanThreads, 0, stream>>>(in, count, partials);
-    SADCS_TRY(cudaGetLastError());
+    SADCS_TRY(launch(scanReduceKernel<Op>, blocks, kScanThreads, 0, stream, in, count, partials));
     SADCS_TRY((deviceScan<Op, false>(partials, partials, blocks, scratch + blocks + 64, nullptr, stream)));
-    scanDownKernel<Op, kInclusive><<<blocks, kScanThreads, 0, stream>>>(in, out, count, partials, totalOut);
+    SADCS_TRY(launch(scanDownKernel<Op, kInclusive>, blocks, kScanThreads, 0, stream, in, out, count, partials, totalOut));
     return cudaGetLastError();
 }
 
-// ---- radix pass ------------------------------------------------------------------------------
+// ---- radix pass (onesweep) ------------------------------------------------------------------
+//
+// One stable counting pass on an 8-bit digit per kernel, reading and writing each element once
+// (Adinets & Merrill's onesweep decomposition): a block takes the next tile in arrival order,
+// ranks its elements stably (warp match on the digit + per-warp counters), publishes its per-digit
+// counts, and looks back over the tiles before it for their running totals (decoupled look-back).
+// The global digit offsets come from one histogram pass made beforehand (for all digits of a sort
+// at once). Tiles are numbered in the order blocks start, so a tile's predecessors are resident or
+// done and the look-back ends; it is still bounded by %globaltimer: past the limit a block sets
+// the error word and stores nothing. Counts stay below 2^30 (flags in the top 2 bits).
 
 constexpr int kSortThreads = 256;
 constexpr int kSortWarps = kSortThreads / 32;
 constexpr int kSortItems = 16;
 constexpr uint32_t kSortTile = kSortThreads * kSortItems;
 constexpr uint32_t kNoDigit = 0x100;
+constexpr uint32_t kStatusAggregate = 1u << 30;
+constexpr uint32_t kStatusPrefix = 2u << 30;
+constexpr uint32_t kStatusValue = (1u << 30) - 1;
+constexpr uint32_t kMaxSortCount = kStatusValue;
+constexpr uint64_t kLookbackLimitNs = 2000000000ull;  // 2 s: far above any real wait
 
-// Shared memory of radixDownsweep for a staged key of KeyBytes bytes.
+__device__ __forceinline__ uint64_t globalTimerNs() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Shared memory of radixOnesweep for a staged key of keyBytes bytes.
 constexpr size_t radixSharedBytes(size_t keyBytes) {
     return kSortTile * keyBytes + kSortTile * 4 + kSortTile + (kSortWarps * 256 + 256 + 256 + 32) * 4 + 64;
 }
 
-template <class Loader>
-__global__ void __launch_bounds__(kSortThreads) radixUpsweep(Loader ld, uint32_t count, uint32_t tiles,
-                                                             uint32_t* __restrict__ hist) {
-    __shared__ uint32_t counts[kSortWarps][256];
-    for (int i = threadIdx.x; i < kSortWarps * 256; i += kSortThreads) (&counts[0][0])[i] = 0;
-    __syncthreads();
-    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint64_t base = static_cast<uint64_t>(blockIdx.x) * kSortTile;
-#pragma unroll 4
-    for (int j = 0; j < kSortItems; j++) {
-        const uint64_t i = base + j * kSortThreads + threadIdx.x;
-        uint32_t d = kNoDigit;
-        if (i < count && !ld.digit(static_cast<uint32_t>(i), d)) d = kNoDigit;
-        const uint32_t peers = __match_any_sync(0xffffffffu, d);
-        if (d != kNoDigit && (peers & ((1u << lane) - 1)) == 0) counts[warp][d] += __popc(peers);
-        __syncwarp();
+// Segments of a pass: element ranges sorted independently, each from its own digit bases, with
+// tiles that never span two segments. The one-segment case is the plain sort.
+struct OneSegment {
+    uint32_t count;
+    __device__ __forceinline__ void locate(uint32_t tile, uint32_t& segment, uint32_t& firstTile, uint32_t& begin,
+                                           uint32_t& size) const {
+        segment = 0;
+        firstTile = 0;
+        begin = 0;
+        size = count;
     }
-    __syncthreads();
-    for (int d = threadIdx.x; d < 256; d += kSortThreads) {
-        uint32_t s = 0;
-#pragma unroll
-        for (int w = 0; w < kSortWarps; w++) s += counts[w][d];
-        hist[static_cast<size_t>(d) * tiles + blockIdx.x] = s;
-    }
-}
+};
 
-template <class Key, class Loader, class Storer>
-__global__ void __launch_bounds__(kSortThreads, 2) radixDownsweep(Loader ld, Storer st, uint32_t count, uint32_t tiles,
-                                                                  const uint32_t* __restrict__ offsets) {
+// Segment s holds elements [elementStart[s], elementStart[s + 1]) and tiles
+// [tileStart[s], tileStart[s + 1]); its digit bases are row s of the digit-base table.
+struct ManySegments {
+    const uint32_t* __restrict__ tileStart;     // [segments + 1]
+    const uint32_t* __restrict__ elementStart;  // [segments + 1]
+    uint32_t segments;
+    __device__ __forceinline__ void locate(uint32_t tile, uint32_t& segment, uint32_t& firstTile, uint32_t& begin,
+                                           uint32_t& size) const {
+        uint32_t lo = 0, hi = segments;  // last s with tileStart[s] <= tile
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (__ldg(tileStart + mid) <= tile) lo = mid; else hi = mid;
+        }
+        segment = lo;
+        firstTile = __ldg(tileStart + lo);
+        begin = __ldg(elementStart + lo);
+        size = __ldg(elementStart + lo + 1) - begin;
+    }
+};
+
+template <class Key, class Loader, class Storer, class Segments = OneSegment>
+__global__ void __launch_bounds__(kSortThreads, 2) radixOnesweep(Loader ld, Storer st, Segments segs,
+                                                                 const uint32_t* __restrict__ digitBase,
+                                                                 uint32_t* __restrict__ status,
+                                                                 uint32_t* __restrict__ tileCounter,
+                                                                 uint32_t* __restrict__ error) {
     extern __shared__ __align__(16) unsigned char smem[];
     Key* sKeys = reinterpret_cast<Key*>(smem);
     uint32_t* sVals = reinterpret_cast<uint32_t*>(sKeys + kSortTile);
@@ -205,13 +236,23 @@ __global__ void __launch_bounds__(kSortThreads, 2) radixDownsweep(Loader ld, Sto
     uint32_t* digitStart = warpCount + kSortWarps * 256;
     uint32_t* digitGlobal = digitStart + 256;
     uint32_t* warpTotals = digitGlobal + 256;
+    __shared__ uint32_t sTile;
+    __shared__ int sFailed;
 
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (threadIdx.x == 0) {
+        sTile = atomicAdd(tileCounter, 1u);
+        sFailed = 0;
+    }
     for (int i = threadIdx.x; i < kSortWarps * 256; i += kSortThreads) warpCount[i] = 0;
-    for (int d = threadIdx.x; d < 256; d += kSortThreads) digitGlobal[d] = offsets[static_cast<size_t>(d) * tiles + blockIdx.x];
     __syncthreads();
+    const uint32_t tile = sTile;
+    uint32_t segment, firstTile, segBegin, segSize;
+    segs.locate(tile, segment, firstTile, segBegin, segSize);
+    const uint32_t localTile = tile - firstTile;
+    const uint32_t count = segSize;
 
-    const uint64_t warpBase = static_cast<uint64_t>(blockIdx.x) * kSortTile + warp * (kSortItems * 32);
+    const uint64_t warpBase = static_cast<uint64_t>(localTile) * kSortTile + warp * (kSortItems * 32);
     uint32_t* myCount = warpCount + warp * 256;
     const uint32_t lt = (1u << lane) - 1;
     Key keys[kSortItems];
@@ -222,7 +263,10 @@ __global__ void __launch_bounds__(kSortThreads, 2) radixDownsweep(Loader ld, Sto
     for (int j = 0; j < kSortItems; j++) {
         const uint64_t i = warpBase + j * 32 + lane;
         uint32_t d = kNoDigit;
-        if (!(i < count && ld.load(static_cast<uint32_t>(i), keys[j], vals[j], d))) d = kNoDigit;
+        if (!(i < count && ld.load(segment, segBegin + static_cast<uint32_t>(i), static_cast<uint32_t>(i), keys[j],
+                                   vals[j], d))) {
+            d = kNoDigit;
+        }
         const uint32_t peers = __match_any_sync(0xffffffffu, d);
         uint32_t before = 0;
         if (d != kNoDigit) before = myCount[d];
@@ -233,53 +277,122 @@ __global__ void __launch_bounds__(kSortThreads, 2) radixDownsweep(Loader ld, Sto
     }
     __syncthreads();
 
-    // Per digit: exclusive prefix over the warps, then the tile's digit starts.
+    // Thread d: the tile's count of digit d, and each warp's exclusive prefix within the tile.
+    const uint32_t d = threadIdx.x;  // kSortThreads == 256
     uint32_t digitTotal = 0;
-    {
-        const uint32_t d = threadIdx.x;  // kSortThreads == 256
-        uint32_t s = 0;
 #pragma unroll
-        for (int w = 0; w < kSortWarps; w++) {
-            const uint32_t c = warpCount[w * 256 + d];
-            warpCount[w * 256 + d] = s;
-            s += c;
-        }
-        digitTotal = s;
+    for (int w = 0; w < kSortWarps; w++) {
+        const uint32_t c = warpCount[w * 256 + d];
+        warpCount[w * 256 + d] = digitTotal;
+        digitTotal += c;
     }
+
+    // Publish, then look back for the running total of every earlier tile.
+    volatile uint32_t* vs = status;
+    uint32_t exclusive = 0;
+    if (tile == firstTile) {
+        vs[static_cast<size_t>(tile) * 256 + d] = kStatusPrefix | digitTotal;
+    } else {
+        vs[static_cast<size_t>(tile) * 256 + d] = kStatusAggregate | digitTotal;
+        uint32_t t = tile;
+        uint64_t waitStart = 0;
+        bool failed = false;
+        while (t > firstTile) {
+            const uint32_t s = vs[static_cast<size_t>(t - 1) * 256 + d];
+            if ((s & ~kStatusValue) == 0) {
+                const uint64_t now = globalTimerNs();
+                if (waitStart == 0) {
+                    waitStart = now;
+                } else if (now - waitStart > kLookbackLimitNs) {
+                    failed = true;
+                    break;
+                }
+                continue;
+            }
+            exclusive += s & kStatusValue;
+            t--;
+            if (s & kStatusPrefix) break;
+        }
+        if (failed) {
+            sFailed = 1;
+        } else {
+            vs[static_cast<size_t>(tile) * 256 + d] = kStatusPrefix | (exclusive + digitTotal);
+        }
+    }
+    digitGlobal[d] = digitBase[static_cast<size_t>(segment) * 256 + d] + exclusive;
     uint32_t tileTotal;
     const uint32_t inclusive = blockInclusiveScan<OpSum>(digitTotal, warpTotals, tileTotal);
-    digitStart[threadIdx.x] = inclusive - digitTotal;
+    digitStart[d] = inclusive - digitTotal;
     __syncthreads();
+    if (sFailed) {
+        if (threadIdx.x == 0) atomicExch(error, 1u);
+        return;
+    }
 
 #pragma unroll
     for (int j = 0; j < kSortItems; j++) {
-        const uint32_t d = rankDigit[j] & 0x1FF;
-        if (d != kNoDigit) {
-            const uint32_t pos = digitStart[d] + warpCount[warp * 256 + d] + (rankDigit[j] >> 9);
+        const uint32_t dj = rankDigit[j] & 0x1FF;
+        if (dj != kNoDigit) {
+            const uint32_t pos = digitStart[dj] + warpCount[warp * 256 + dj] + (rankDigit[j] >> 9);
             sKeys[pos] = keys[j];
             sVals[pos] = vals[j];
-            sDig[pos] = static_cast<uint8_t>(d);
+            sDig[pos] = static_cast<uint8_t>(dj);
         }
     }
     __syncthreads();
 
     for (uint32_t i = threadIdx.x; i < tileTotal; i += kSortThreads) {
-        const uint32_t d = sDig[i];
-        st.store(digitGlobal[d] + i - digitStart[d], sKeys[i], sVals[i]);
+        const uint32_t dj = sDig[i];
+        st.store(segment, digitGlobal[dj] + i - digitStart[dj], sKeys[i], sVals[i]);
     }
 }
 
+// Digit histograms of a sort, all passes at once: hist[p * 256 + digit] (zeroed by the caller).
+template <class Key>
+__global__ void __launch_bounds__(256) radixHistogram(const Key* __restrict__ keys, uint32_t count, int beginBit,
+                                                      int passes, uint32_t* __restrict__ hist) {
+    __shared__ uint32_t h[8][256];
+    for (int i = threadIdx.x; i < 8 * 256; i += blockDim.x) (&h[0][0])[i] = 0;
+    __syncthreads();
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t lt = (1u << lane) - 1;
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    for (uint64_t base = static_cast<uint64_t>(blockIdx.x) * blockDim.x; base < count; base += stride) {
+        const uint64_t i = base + threadIdx.x;
+        const bool valid = i < count;
+        const Key k = valid ? keys[i] : Key(0);
+        for (int p = 0; p < passes; p++) {
+            const uint32_t dg = valid ? static_cast<uint32_t>(k >> (beginBit + 8 * p)) & 0xFF : kNoDigit;
+            const uint32_t peers = __match_any_sync(0xffffffffu, dg);
+            if (dg != kNoDigit && (peers & lt) == 0) atomicAdd(&h[p][dg], static_cast<uint32_t>(__popc(peers)));
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < passes * 256; i += blockDim.x) {
+        const uint32_t v = (&h[0][0])[i];
+        if (v) atomicAdd(hist + i, v);
+    }
+}
+
+// Exclusive scan of each 256-entry row of hist, in place. One block per row.
+__global__ void __launch_bounds__(256) radixDigitBase(uint32_t* __restrict__ hist) {
+    __shared__ uint32_t warpTotals[32];
+    uint32_t* row = hist + blockIdx.x * 256;
+    const uint32_t v = row[threadIdx.x];
+    uint32_t total;
+    const uint32_t inclusive = blockInclusiveScan<OpSum>(v, warpTotals, total);
+    row[threadIdx.x] = inclusive - v;
+}
+
 // Keys and values of a sort pass.
+// Loaders get (segment, element index in the pass, index within the segment); storers get the
+// segment and the output position.
 template <class Key>
 struct SortLoader {
     const Key* __restrict__ keys;
     const uint32_t* __restrict__ vals;
     int shift;
-    __device__ __forceinline__ bool digit(uint32_t i, uint32_t& d) const {
-        d = static_cast<uint32_t>(keys[i] >> shift) & 0xFF;
-        return true;
-    }
-    __device__ __forceinline__ bool load(uint32_t i, Key& k, uint32_t& v, uint32_t& d) const {
+    __device__ __forceinline__ bool load(uint32_t, uint32_t i, uint32_t, Key& k, uint32_t& v, uint32_t& d) const {
         k = keys[i];
         v = vals[i];
         d = static_cast<uint32_t>(k >> shift) & 0xFF;
@@ -291,50 +404,83 @@ template <class Key>
 struct SortStorer {
     Key* __restrict__ keys;
     uint32_t* __restrict__ vals;
-    __device__ __forceinline__ void store(uint32_t pos, Key k, uint32_t v) const {
-        keys[pos] = k;
-        vals[pos] = v;
+    uint32_t limit;
+    __device__ __forceinline__ void store(uint32_t, uint32_t pos, Key k, uint32_t v) const {
+        if (pos < limit) {  // always, unless an earlier pass's look-back timed out
+            keys[pos] = k;
+            vals[pos] = v;
+        }
     }
 };
 
-// Words of scratch one radix pass over count elements needs (histograms + their scan).
+// Words of scratch a radix sort (or one filtered pass) over count elements needs:
+// 8 x 256 digit bases, the tile status words, the tile counter and the error word.
 inline size_t radixScratchWords(uint64_t count) {
     const uint64_t tiles = (count + kSortTile - 1) / kSortTile;
-    return static_cast<size_t>(tiles * 256) + scanScratchWords(tiles * 256) + 64;
+    return 8 * 256 + static_cast<size_t>(tiles) * 256 + 64;
 }
 
-template <class Key, class Loader, class Storer>
-cudaError_t radixPass(const Loader& ld, const Storer& st, uint32_t count, uint32_t* scratch, cudaStream_t stream) {
-    if (count == 0) return cudaSuccess;
-    const uint32_t tiles = ceilDiv(count, kSortTile);
-    uint32_t* hist = scratch;
-    uint32_t* scanScratch = scratch + static_cast<size_t>(tiles) * 256 + 32;
-    radixUpsweep<Loader><<<tiles, kSortThreads, 0, stream>>>(ld, count, tiles, hist);
-    SADCS_TRY(cudaGetLastError());
-    SADCS_TRY((deviceScan<OpSum, false>(hist, hist, tiles * 256u, scanScratch, nullptr, stream)));
+// The error word of a RadixScratch built on scratchWords.
+inline uint32_t* radixErrorWord(uint32_t* scratchWords) {
+    return scratchWords + 8 * 256 + 1;
+}
+
+struct RadixScratch {
+    uint32_t* digitBase;  // [8][256]
+    uint32_t* status;     // [tiles][256]
+    uint32_t* control;    // [0] tile counter, [1] error word
+    explicit RadixScratch(uint32_t* s, uint64_t count) {
+        digitBase = s;
+        control = s + 8 * 256;
+        status = control + 64;
+        (void)count;
+    }
+};
+
+// One pass over `tiles` tiles (ceilDiv(count, kSortTile) for one segment; the segment table's total
+// otherwise). count bounds the elements of the pass (all segments together).
+template <class Key, class Loader, class Storer, class Segments = OneSegment>
+cudaError_t radixOnesweepPass(const Loader& ld, const Storer& st, const Segments& segs, uint32_t count,
+                              uint32_t tiles, const uint32_t* digitBase, const RadixScratch& scratch,
+                              cudaStream_t stream) {
+    if (count == 0 || tiles == 0) return cudaSuccess;
+    if (count > kMaxSortCount) return cudaErrorInvalidValue;
+    // status words and the tile counter start at zero; the error word is kept.
+    SADCS_TRY(cudaMemsetAsync(scratch.status, 0, static_cast<size_t>(tiles) * 256 * 4, stream));
+    SADCS_TRY(cudaMemsetAsync(scratch.control, 0, 4, stream));
     constexpr size_t shared = radixSharedBytes(sizeof(Key));
     // The opt-in above 48 KiB of dynamic shared memory is per function and per device.
     static uint64_t configured = 0;
     int device = 0;
     SADCS_TRY(cudaGetDevice(&device));
     if (!(configured >> (device & 63) & 1)) {
-        SADCS_TRY(cudaFuncSetAttribute(radixDownsweep<Key, Loader, Storer>,
+        SADCS_TRY(cudaFuncSetAttribute(radixOnesweep<Key, Loader, Storer, Segments>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(shared)));
         configured |= uint64_t(1) << (device & 63);
     }
-    radixDownsweep<Key, Loader, Storer><<<tiles, kSortThreads, shared, stream>>>(ld, st, count, tiles, hist);
-    return cudaGetLastError();
+    return launch(radixOnesweep<Key, Loader, Storer, Segments>, tiles, kSortThreads, shared, stream, ld, st, segs,
+                  digitBase, scratch.status, scratch.control, scratch.control + 1);
 }
 
 // Stable LSD sort of (keys, vals) over bits [beginBit, endBit), ping-ponging with the alternates.
 // On return keys/vals point at the sorted data (swapped with the alternates if the pass count is odd).
+// The error word (scratch control[1]) is left nonzero if a look-back timed out.
 template <class Key>
 cudaError_t radixSortPairs(Key*& keys, Key*& keysAlt, uint32_t*& vals, uint32_t*& valsAlt, uint32_t count,
-                           int beginBit, int endBit, uint32_t* scratch, cudaStream_t stream) {
-    for (int bit = beginBit; bit < endBit; bit += 8) {
-        SortLoader<Key> ld{keys, vals, bit};
-        SortStorer<Key> st{keysAlt, valsAlt};
-        SADCS_TRY((radixPass<Key>(ld, st, count, scratch, stream)));
+                           int beginBit, int endBit, uint32_t* scratchWords, cudaStream_t stream) {
+    if (count <= 1 || endBit <= beginBit) return cudaSuccess;
+    const RadixScratch scratch(scratchWords, count);
+    const int passes = (endBit - beginBit + 7) / 8;
+    SADCS_TRY(cudaMemsetAsync(scratch.digitBase, 0, static_cast<size_t>(passes) * 256 * 4, stream));
+    const uint32_t histBlocks = std::min<uint32_t>(ceilDiv(count, 256 * 16), 148 * 8);
+    SADCS_TRY(launch(radixHistogram<Key>, histBlocks, 256, 0, stream, keys, count, beginBit, passes,
+                     scratch.digitBase));
+    SADCS_TRY(launch(radixDigitBase, passes, 256, 0, stream, scratch.digitBase));
+    for (int p = 0; p < passes; p++) {
+        SortLoader<Key> ld{keys, vals, beginBit + 8 * p};
+        SortStorer<Key> st{keysAlt, valsAlt, count};
+        SADCS_TRY((radixOnesweepPass<Key>(ld, st, OneSegment{count}, count, ceilDiv(count, kSortTile),
+                                          scratch.digitBase + p * 256, scratch, stream)));
         Key* k = keys;
         keys = keysAlt;
         keysAlt = k;

@@ -28,8 +28,9 @@ struct RankBuffers {
     uint32_t* grp;
     uint32_t* aux1;
     uint32_t* aux2;
-    uint32_t* scratch;  // sort/scan scratch words
-    uint32_t* counter;  // one device word
+    uint32_t* scratch;      // radix scratch words (radixScratchWords(m))
+    uint32_t* scanScratch;  // scan scratch words (scanScratchWords(m))
+    uint32_t* counter;      // one device word
 };
 
 constexpr uint32_t kCharsPerPass = 7;
@@ -47,26 +48,45 @@ __global__ void rankInitList(uint32_t* __restrict__ lst, uint32_t m) {
     if (i < m) lst[i] = i;
 }
 
-// doubling == 0: character key at depth; otherwise 1 + rank at p + h.
-__global__ void rankMakeKeys(const uint8_t* __restrict__ text, const uint32_t* __restrict__ ranks, uint32_t n,
+// doubling == 0: character key at depth; otherwise 1 + rank at p + h. Keys stop at the end of
+// the suffix's own text.
+__global__ void rankMakeKeys(const uint8_t* __restrict__ text, const uint32_t* __restrict__ ranks, TextSet texts,
                              const uint32_t* __restrict__ lst, uint64_t* __restrict__ key, uint32_t u,
                              uint32_t offset, int doubling) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= u) return;
     const uint32_t p = samplePosition(lst[i]);
+    const uint32_t end = texts.endOf(p);
+    const uint64_t q = static_cast<uint64_t>(p) + offset;
     if (doubling) {
-        const uint64_t q = static_cast<uint64_t>(p) + offset;
-        key[i] = q < n ? static_cast<uint64_t>(ranks[pack(static_cast<uint32_t>(q))]) + 1 : 0;
+        key[i] = q < end ? static_cast<uint64_t>(ranks[pack(static_cast<uint32_t>(q))]) + 1 : 0;
     } else {
-        const uint64_t q = static_cast<uint64_t>(p) + offset;
-        key[i] = q < n ? charKey(text, n, static_cast<uint32_t>(q)) : 0;
+        key[i] = q < end ? charKey(text, end, static_cast<uint32_t>(q)) : 0;
+    }
+}
+
+// Several texts: the list holds every live sample (a sample position inside its text) in text
+// order, and each starts in its text's group: ranks[t] = live samples of the texts before.
+__global__ void rankInitTexts(TextSet texts, const uint32_t* __restrict__ sampleBase, uint32_t slots,
+                              uint32_t* __restrict__ lst, uint32_t* __restrict__ ranks) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= slots) return;
+    const uint32_t p = samplePosition(t);
+    const uint32_t j = texts.textOf(p);
+    const uint32_t start = texts.startOf(j);
+    if (p >= start && p < texts.endOfText(j)) {
+        const uint32_t base = sampleBase[j];
+        lst[base + (t - (start / kV) * kK)] = t;
+        ranks[t] = base;
+    } else {
+        ranks[t] = 0;
     }
 }
 
 __global__ void rankGatherGroups(const uint32_t* __restrict__ ranks, const uint32_t* __restrict__ lst,
-                                 uint32_t* __restrict__ grp, uint32_t u) {
+                                 uint32_t* __restrict__ grp, uint32_t u, uint32_t m) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < u) grp[i] = ranks[lst[i]];
+    if (i < u) grp[i] = lst[i] < m ? ranks[lst[i]] : 0;
 }
 
 // aux1[i] = grp[i] - i at the first element of an old group (>= 0: every listed element before it
@@ -93,10 +113,10 @@ __global__ void rankNewHeads(const uint32_t* __restrict__ grp, const uint64_t* _
 // Writes the ids; flags[i] = 1 for elements still in a group of two or more.
 __global__ void rankStore(const uint32_t* __restrict__ grp, const uint64_t* __restrict__ key,
                           const uint32_t* __restrict__ ids, const uint32_t* __restrict__ lst,
-                          uint32_t* __restrict__ ranks, uint32_t* __restrict__ flags, uint32_t u) {
+                          uint32_t* __restrict__ ranks, uint32_t* __restrict__ flags, uint32_t u, uint32_t m) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= u) return;
-    ranks[lst[i]] = ids[i];
+    if (lst[i] < m) ranks[lst[i]] = ids[i];
     const bool single = newHead(grp, key, i) && (i + 1 == u || newHead(grp, key, i + 1));
     flags[i] = single ? 0 : 1;
 }
@@ -126,60 +146,64 @@ struct RankStats {
 };
 
 __global__ void rankGatherGroupKeys(const uint32_t* __restrict__ ranks, const uint32_t* __restrict__ lst,
-                                    uint64_t* __restrict__ key, uint32_t u) {
+                                    uint64_t* __restrict__ key, uint32_t u, uint32_t m) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < u) key[i] = ranks[lst[i]];
+    if (i < u) key[i] = lst[i] < m ? ranks[lst[i]] : 0;
 }
 
-// Ranks the m = sampleSize(n) sample suffixes of text into ranks[0, m) (ranks zeroed by the caller,
-// including kRankPad entries past m). hostCounter: page-locked word for the per-pass count.
-inline cudaError_t rankSample(const uint8_t* text, uint32_t n, uint32_t* ranks, RankBuffers b, uint32_t* hostCounter,
-                              cudaStream_t stream, RankStats& stats) {
-    const uint32_t m = static_cast<uint32_t>(sampleSize(n));
-    if (m == 0) return cudaSuccess;
+// Ranks the live sample suffixes of the texts. slots = rank entries (sample positions of the whole
+// concatenation); live = live samples; sampleBase (device, per text) is used with several texts.
+// Ranks of live samples end up in [0, live), text by text; ranks are zeroed by the caller for one
+// text (and kRankPad entries past slots always). hostCounter: two page-locked words.
+inline cudaError_t rankSample(const uint8_t* text, const TextSet& texts, uint32_t slots, uint32_t live,
+                              const uint32_t* sampleBase, uint32_t longest, uint32_t* ranks, RankBuffers b,
+                              uint32_t* hostCounter, cudaStream_t stream, RankStats& stats) {
+    if (live == 0) return cudaSuccess;
     uint32_t* cur = b.lst[0];
     uint32_t* alt = b.lst[1];
-    rankInitList<<<blocks256(m), 256, 0, stream>>>(cur, m);
-    SADCS_TRY(cudaGetLastError());
-    uint32_t u = m;
+    if (texts.count <= 1) {
+        SADCS_TRY(launch(rankInitList, blocks256(live), 256, 0, stream, cur, live));
+    } else {
+        SADCS_TRY(launch(rankInitTexts, blocks256(slots), 256, 0, stream, texts, sampleBase, slots, cur, ranks));
+    }
+    uint32_t* error = radixErrorWord(b.scratch);
+    SADCS_TRY(cudaMemsetAsync(error, 0, sizeof(uint32_t), stream));
+    uint32_t u = live;
     uint64_t depth = 0;
-    bool first = true;
-    const int rankBits = bitWidth(static_cast<uint64_t>(m) + 1);
+    bool first = texts.count <= 1;  // one text: everything starts in one group, no group sort
+    const int rankBits = bitWidth(static_cast<uint64_t>(live) + 1);
     while (u > 0) {
         const bool doubling = depth >= kV;
         const uint32_t offset = doubling ? static_cast<uint32_t>((depth / kV) * kV) : static_cast<uint32_t>(depth);
-        if (depth > static_cast<uint64_t>(n) + 2 * kV) return cudaErrorUnknown;  // invariant: groups share < n chars
+        if (depth > static_cast<uint64_t>(longest) + 2 * kV) return cudaErrorUnknown;  // groups share < n chars
 
         uint32_t* lst = cur;
         uint32_t* lstAlt = alt;
         uint64_t* key = b.key[0];
         uint64_t* keyAlt = b.key[1];
-        rankMakeKeys<<<blocks256(u), 256, 0, stream>>>(text, ranks, n, lst, key, u, offset, doubling ? 1 : 0);
-        SADCS_TRY(cudaGetLastError());
+        SADCS_TRY(launch(rankMakeKeys, blocks256(u), 256, 0, stream, text, ranks, texts, lst, key, u, offset,
+                         doubling ? 1 : 0));
         SADCS_TRY(radixSortPairs<uint64_t>(key, keyAlt, lst, lstAlt, u, 0, doubling ? rankBits : 64, b.scratch, stream));
         if (!first) {
             // Stably by the old group id (the list keeps whole groups in id order), then recompute
             // the subkeys in the new order; the subkey buffer is free for the group keys meanwhile.
-            rankGatherGroupKeys<<<blocks256(u), 256, 0, stream>>>(ranks, lst, key, u);
-            SADCS_TRY(cudaGetLastError());
+            SADCS_TRY(launch(rankGatherGroupKeys, blocks256(u), 256, 0, stream, ranks, lst, key, u, slots));
             SADCS_TRY(radixSortPairs<uint64_t>(key, keyAlt, lst, lstAlt, u, 0, rankBits, b.scratch, stream));
-            rankMakeKeys<<<blocks256(u), 256, 0, stream>>>(text, ranks, n, lst, key, u, offset, doubling ? 1 : 0);
-            SADCS_TRY(cudaGetLastError());
+            SADCS_TRY(launch(rankMakeKeys, blocks256(u), 256, 0, stream, text, ranks, texts, lst, key, u, offset,
+                             doubling ? 1 : 0));
         }
-        rankGatherGroups<<<blocks256(u), 256, 0, stream>>>(ranks, lst, b.grp, u);
-        rankOldHeads<<<blocks256(u), 256, 0, stream>>>(b.grp, b.aux1, u);
-        SADCS_TRY(cudaGetLastError());
-        SADCS_TRY((deviceScan<OpMax, true>(b.aux1, b.aux1, u, b.scratch, nullptr, stream)));
-        rankNewHeads<<<blocks256(u), 256, 0, stream>>>(b.grp, key, b.aux1, b.aux2, u);
-        SADCS_TRY(cudaGetLastError());
-        SADCS_TRY((deviceScan<OpMax, true>(b.aux2, b.aux2, u, b.scratch, nullptr, stream)));
-        rankStore<<<blocks256(u), 256, 0, stream>>>(b.grp, key, b.aux2, lst, ranks, b.aux1, u);
-        SADCS_TRY(cudaGetLastError());
-        SADCS_TRY((deviceScan<OpSum, false>(b.aux1, b.aux2, u, b.scratch, b.counter, stream)));
-        rankCompact<<<blocks256(u), 256, 0, stream>>>(lst, b.aux1, b.aux2, lstAlt, u);
-        SADCS_TRY(cudaGetLastError());
+        SADCS_TRY(launch(rankGatherGroups, blocks256(u), 256, 0, stream, ranks, lst, b.grp, u, slots));
+        SADCS_TRY(launch(rankOldHeads, blocks256(u), 256, 0, stream, b.grp, b.aux1, u));
+        SADCS_TRY((deviceScan<OpMax, true>(b.aux1, b.aux1, u, b.scanScratch, nullptr, stream)));
+        SADCS_TRY(launch(rankNewHeads, blocks256(u), 256, 0, stream, b.grp, key, b.aux1, b.aux2, u));
+        SADCS_TRY((deviceScan<OpMax, true>(b.aux2, b.aux2, u, b.scanScratch, nullptr, stream)));
+        SADCS_TRY(launch(rankStore, blocks256(u), 256, 0, stream, b.grp, key, b.aux2, lst, ranks, b.aux1, u, slots));
+        SADCS_TRY((deviceScan<OpSum, false>(b.aux1, b.aux2, u, b.scanScratch, b.counter, stream)));
+        SADCS_TRY(launch(rankCompact, blocks256(u), 256, 0, stream, lst, b.aux1, b.aux2, lstAlt, u));
         SADCS_TRY(cudaMemcpyAsync(hostCounter, b.counter, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+        SADCS_TRY(cudaMemcpyAsync(hostCounter + 1, error, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
         SADCS_TRY(cudaStreamSynchronize(stream));
+        if (hostCounter[1]) return cudaErrorLaunchTimeout;  // a radix look-back gave up
         u = *hostCounter;
         cur = lstAlt;
         alt = lst;

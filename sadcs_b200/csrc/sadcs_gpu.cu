@@ -15,8 +15,11 @@
 #include <cstdio>
 #include <cstring>
 #include <new>
+#include <string>
+#include <vector>
 
 #include "bwt.cuh"
+#include "check.cuh"
 #include "classes.cuh"
 #include "common.cuh"
 #include "merge.cuh"
@@ -49,38 +52,120 @@ double secondsSince(std::chrono::steady_clock::time_point start) {
 constexpr int64_t kMemoryReserve = int64_t(256) << 20;          // gpusa.h:82
 constexpr int64_t kMaxInt32Text = int64_t(INT32_MAX) - 1024;    // src/cpu/dcsort.h:21
 constexpr int64_t kMaxText = (int64_t(1) << 32) - 256;
+constexpr uint32_t kMaxTexts = 1u << 20;
 
 size_t align256(size_t bytes) {
     return (bytes + 255) & ~size_t(255);
 }
 
-// Byte offsets of every buffer of a construction of n bytes, and the peaks.
-struct Layout {
-    uint64_t n = 0, m = 0;
-    size_t text = 0, ranks = 0;
-    // ranking region
-    size_t lst0 = 0, lst1 = 0, key0 = 0, key1 = 0, grp = 0, aux1 = 0, aux2 = 0, rankScratch = 0, counter = 0;
-    // class + merge region (overlaps the ranking region)
-    size_t lists = 0, classScratch = 0, splitters = 0, rows = 0, sa = 0, bwt = 0, mergeCounter = 0;
-    size_t rankingEnd = 0, classEnd = 0, mergeEnd = 0, peak = 0;
+// Host plan of one construction: a batch of texts (one text is a batch of one). Text j is placed
+// at start[j], a multiple of 32, and ends at end[j]; empty texts are left out by the caller.
+struct Batch {
+    uint32_t count = 0;
+    std::vector<uint64_t> lengths;
+    std::vector<uint32_t> start, end, sampleBase, outBase;  // outBase: count + 1 entries
+    uint64_t span = 0;     // bytes of the concatenation, gaps included (a multiple of 32)
+    uint64_t slots = 0;    // rank entries: sample positions of the whole span
+    uint64_t live = 0;     // sample positions inside texts
+    uint64_t outputs = 0;  // total length: SA entries and BWT bytes
+    uint64_t longest = 0;
+    ClassPlan classes;
+    std::vector<uint32_t> classTables;
     MergePlan merge;
 };
 
-Layout planLayout(uint64_t n, bool internalSa, bool internalBwt) {
+bool planBatch(const uint64_t* lengths, uint32_t count, Batch& b) {
+    b.count = count;
+    b.lengths.assign(lengths, lengths + count);
+    b.start.resize(count);
+    b.end.resize(count);
+    b.sampleBase.resize(count);
+    b.outBase.resize(count + 1);
+    uint64_t at = 0, live = 0, outputs = 0;
+    for (uint32_t j = 0; j < count; j++) {
+        b.start[j] = static_cast<uint32_t>(at);
+        b.end[j] = static_cast<uint32_t>(at + lengths[j]);
+        b.sampleBase[j] = static_cast<uint32_t>(live);
+        b.outBase[j] = static_cast<uint32_t>(outputs);
+        live += sampleSize(lengths[j]);
+        outputs += lengths[j];
+        b.longest = std::max<uint64_t>(b.longest, lengths[j]);
+        at += (lengths[j] + kV - 1) / kV * kV;
+        if (at > static_cast<uint64_t>(kMaxText)) return false;
+    }
+    b.outBase[count] = static_cast<uint32_t>(outputs);
+    b.span = at;
+    b.slots = (at / kV) * kK;
+    b.live = live;
+    b.outputs = outputs;
+    b.classTables.assign(ClassTables::words(count), 0);
+    planClasses(lengths, count, b.classTables.data(), b.classes);
+    b.merge = planMerge(b.classes.start);
+    return true;
+}
+
+// Words of the per-construction tables: start, end, sampleBase, outBase, rowZero, the class
+// tables and (several texts) the text of every 32-byte block.
+size_t metaWords(uint32_t count, uint64_t span) {
+    return 5 * static_cast<size_t>(count) + 1 + ClassTables::words(count) + (count > 1 ? span / kV + 1 : 0) + 16;
+}
+
+// Byte offsets of every buffer of a construction, and the peaks.
+struct Layout {
+    size_t text = 0, ranks = 0, meta = 0;
+    // ranking region (the packed upload of a batch is staged at its start)
+    size_t lst0 = 0, lst1 = 0, key0 = 0, key1 = 0, grp = 0, aux1 = 0, aux2 = 0, rankScratch = 0, scanScratch = 0;
+    size_t counter = 0;
+    // class + merge region (overlaps the ranking region)
+    size_t lists = 0, classScratch = 0, splitters = 0, rows = 0, sa = 0, bwt = 0, mergeCounter = 0;
+    size_t rankingEnd = 0, classEnd = 0, mergeEnd = 0, peak = 0;
+};
+
+// Sizes a layout depends on; for a context they are upper bounds over every batch it admits.
+struct Extent {
+    uint64_t span, slots, live, outputs, largestClass, splitterWords, rows;
+    uint32_t count;
+};
+
+Extent extentOf(const Batch& b) {
+    return {b.span, b.slots, b.live, b.outputs, b.classes.largest, b.merge.splitterWords, b.merge.rows, b.count};
+}
+
+// Bounds for any batch of at most `texts` texts and `total` bytes.
+Extent extentBound(uint64_t total, uint32_t texts) {
+    Extent e{};
+    e.count = std::max<uint32_t>(texts, 1);
+    e.span = (total + static_cast<uint64_t>(kV - 1) * e.count + kV - 1) / kV * kV;
+    e.slots = (e.span / kV) * kK;
+    e.live = std::min<uint64_t>(total, (total / kV) * kK + static_cast<uint64_t>(kK) * e.count);
+    e.outputs = total;
+    e.largestClass = e.live;
+    uint64_t words = 0, rows = 0, level = total;
+    while (level > kMergeCap) {
+        const uint64_t next = level / kMergeG + kClasses;
+        words += next + 64;
+        rows += (next + kMergeR - 1) / kMergeR + 1;
+        level = next;
+    }
+    e.splitterWords = words;
+    e.rows = rows;
+    return e;
+}
+
+Layout planLayout(const Extent& x, bool internalSa, bool internalBwt) {
     Layout L;
-    L.n = n;
-    L.m = sampleSize(n);
-    const uint64_t m = L.m;
     size_t at = 0;
     auto take = [&at](size_t bytes) {
         const size_t offset = at;
         at += align256(bytes);
         return offset;
     };
-    L.text = take(n + kTextPad);
-    L.ranks = take(4 * (m + kRankPad));
+    L.text = take(x.span + kTextPad);
+    L.ranks = take(4 * (x.slots + kRankPad));
+    L.meta = take(4 * metaWords(x.count, x.span));
     const size_t persistent = at;
 
+    const uint64_t m = x.live;
     L.lst0 = take(4 * m);
     L.lst1 = take(4 * m);
     L.key0 = take(8 * m);
@@ -88,27 +173,43 @@ Layout planLayout(uint64_t n, bool internalSa, bool internalBwt) {
     L.grp = take(4 * m);
     L.aux1 = take(4 * m);
     L.aux2 = take(4 * m);
-    L.rankScratch = take(4 * std::max(radixScratchWords(m), scanScratchWords(m)));
+    L.rankScratch = take(4 * radixScratchWords(m));
+    L.scanScratch = take(4 * scanScratchWords(m));
     L.counter = take(256);
-    L.rankingEnd = at;
+    L.rankingEnd = std::max(at, persistent + align256(x.outputs));
 
     at = persistent;
-    const ClassLayout classes = classLayout(n);
-    uint64_t largest = 0;
-    for (int d = 0; d < kClasses; d++) largest = std::max<uint64_t>(largest, classes.start[d + 1] - classes.start[d]);
-    L.lists = take(4 * n);
-    L.classScratch = take(4 * radixScratchWords(largest + 1));
+    L.lists = take(4 * x.outputs);
+    L.classScratch = take(4 * classScratchWords(x.span, x.count));
     L.classEnd = at;
     at = L.classScratch;  // the merge reuses the class scratch
-    L.merge = planMerge(classes.start);
-    L.splitters = take(4 * L.merge.splitterWords);
-    L.rows = take(sizeof(MergeRow) * (L.merge.rows + 1));
+    L.splitters = take(4 * x.splitterWords);
+    L.rows = take(sizeof(MergeRow) * (x.rows + 1));
     L.mergeCounter = take(256);
-    L.sa = internalSa ? take(4 * n) : 0;
-    L.bwt = internalBwt ? take(n) : 0;
+    L.sa = internalSa ? take(4 * x.outputs) : 0;
+    L.bwt = internalBwt ? take(x.outputs) : 0;
     L.mergeEnd = at;
     L.peak = std::max({L.rankingEnd, L.classEnd, L.mergeEnd});
     return L;
+}
+
+// Copies the packed texts (text j at packedOffset[j]) to their 32-aligned places and zeroes every
+// gap and the padding after the last text. One block per text.
+__global__ void placeTexts(const uint8_t* __restrict__ packed, const uint32_t* __restrict__ start,
+                           const uint32_t* __restrict__ end, const uint32_t* __restrict__ packedOffset, uint32_t count,
+                           uint32_t span, uint8_t* __restrict__ text) {
+    const uint32_t j = blockIdx.x;
+    const uint32_t s = start[j], e = end[j], next = j + 1 < count ? start[j + 1] : span + kTextPad;
+    const uint8_t* src = packed + packedOffset[j];
+    for (uint32_t i = s + threadIdx.x; i < next; i += blockDim.x) text[i] = i < e ? src[i - s] : 0;
+}
+
+// blockText[k] = the text whose range contains or precedes the 32-byte block k. One block per text.
+__global__ void fillBlockText(const uint32_t* __restrict__ start, uint32_t count, uint32_t span,
+                              uint32_t* __restrict__ blockText) {
+    const uint32_t j = blockIdx.x;
+    const uint32_t first = start[j] / kV, last = (j + 1 < count ? start[j + 1] : span) / kV + (j + 1 < count ? 0 : 1);
+    for (uint32_t k = first + threadIdx.x; k < last; k += blockDim.x) blockText[k] = j;
 }
 
 }  // namespace
@@ -116,10 +217,12 @@ Layout planLayout(uint64_t n, bool internalSa, bool internalBwt) {
 struct sadcs_gpu_context {
     int device = 0;
     uint64_t capacity = 0;
+    uint32_t maxTexts = 1;
     size_t slabBytes = 0;
     uint8_t* slab = nullptr;
     cudaStream_t stream = nullptr;
-    uint32_t* hostWords = nullptr;  // page-locked
+    uint32_t* hostWords = nullptr;  // page-locked: counters and the per-construction tables
+    size_t hostWordCount = 0;
     cudaEvent_t events[6] = {};
 };
 
@@ -175,20 +278,23 @@ int queryDevice(sadcs_gpu_device* device) {
     return SADCS_OK;
 }
 
-int createContext(int64_t capacity, sadcs_gpu_context** out) {
+size_t contextBytes(int64_t capacity, uint32_t texts) {
+    return planLayout(extentBound(static_cast<uint64_t>(capacity), texts), true, true).peak;
+}
+
+int createContext(int64_t capacity, uint32_t texts, sadcs_gpu_context** out) {
     *out = nullptr;
     sadcs_gpu_device device;
     if (const int status = queryDevice(&device); status != SADCS_OK) return status;
-    if (capacity < 0 || capacity > kMaxText) {
-        setError("capacity %lld out of range (0 to %lld bytes)", static_cast<long long>(capacity),
-                 static_cast<long long>(kMaxText));
+    if (capacity < 0 || capacity > kMaxText || texts == 0 || texts > kMaxTexts) {
+        setError("capacity %lld bytes / %u texts out of range (0 to %lld bytes, 1 to %u texts)",
+                 static_cast<long long>(capacity), texts, static_cast<long long>(kMaxText), kMaxTexts);
         return SADCS_FAILED;
     }
-    const Layout L = planLayout(static_cast<uint64_t>(capacity), true, true);
-    const int64_t peak = static_cast<int64_t>(L.peak);
-    if (peak + kMemoryReserve > device.free_bytes) {
+    const size_t bytes = contextBytes(capacity, texts);
+    if (static_cast<int64_t>(bytes) + kMemoryReserve > device.free_bytes) {
         setError("needs %lld MiB of device memory plus %lld MiB reserve, %lld MiB free",
-                 static_cast<long long>(peak >> 20), static_cast<long long>(kMemoryReserve >> 20),
+                 static_cast<long long>(bytes >> 20), static_cast<long long>(kMemoryReserve >> 20),
                  static_cast<long long>(device.free_bytes >> 20));
         return SADCS_NOT_ENOUGH_MEMORY;
     }
@@ -199,10 +305,13 @@ int createContext(int64_t capacity, sadcs_gpu_context** out) {
     }
     cudaGetDevice(&c->device);
     c->capacity = static_cast<uint64_t>(capacity);
-    c->slabBytes = L.peak;
+    c->maxTexts = texts;
+    c->slabBytes = bytes;
+    // counters, then the host copy of the tables (without the block map, built on the device)
+    c->hostWordCount = 64 + metaWords(texts, 0) + 2 * static_cast<size_t>(texts) + 64;
     cudaError_t error;
     if ((error = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess ||
-        (error = cudaMallocHost(&c->hostWords, 256)) != cudaSuccess ||
+        (error = cudaMallocHost(&c->hostWords, 4 * c->hostWordCount)) != cudaSuccess ||
         (error = cudaMalloc(&c->slab, std::max<size_t>(c->slabBytes, 256))) != cudaSuccess) {
         const int status = failed("creating the context", error);
         destroyContext(c);
@@ -234,45 +343,112 @@ float elapsedMs(cudaEvent_t a, cudaEvent_t b) {
     return ms;
 }
 
-// One construction on the context's slab. Either hostText or deviceText is given. Outputs: device
-// pointers (outSa/outBwt, caller-owned) or, when null and wanted, the slab's internal buffers,
-// returned through internalSa/internalBwt for the caller to download.
-int construct(sadcs_gpu_context* c, const uint8_t* hostText, const uint8_t* deviceText, uint64_t n, bool wantSa,
-              bool wantBwt, uint32_t* outSa, uint8_t* outBwt, cudaStream_t stream, sadcs_gpu_stats& s,
-              uint32_t*& internalSa, uint8_t*& internalBwt, uint32_t& row0) {
-    if (n > c->capacity) {
-        setError("input of %llu bytes exceeds the context's capacity of %llu bytes", static_cast<unsigned long long>(n),
-                 static_cast<unsigned long long>(c->capacity));
+// Where a construction's inputs come from and its outputs go.
+struct Io {
+    const uint8_t* hostText = nullptr;    // packed host texts, or
+    const uint8_t* deviceText = nullptr;  // packed device texts
+    bool wantSa = false, wantBwt = false;
+    uint32_t* outSa = nullptr;            // device outputs (caller-owned), or null for the slab's
+    uint8_t* outBwt = nullptr;
+    // results
+    uint32_t* deviceSa = nullptr;         // where the SA / BWT ended up
+    uint8_t* deviceBwt = nullptr;
+    uint32_t* rowZero = nullptr;          // device, per text
+};
+
+// One construction of a batch on the context's slab.
+int construct(sadcs_gpu_context* c, const Batch& b, Io& io, cudaStream_t stream, sadcs_gpu_stats& s) {
+    if (b.outputs > c->capacity || b.count > c->maxTexts) {
+        setError("input of %llu bytes in %u texts exceeds the context's capacity of %llu bytes / %u texts",
+                 static_cast<unsigned long long>(b.outputs), b.count, static_cast<unsigned long long>(c->capacity),
+                 c->maxTexts);
         return SADCS_NOT_ENOUGH_MEMORY;
     }
-    const Layout L = planLayout(n, wantSa && !outSa, wantBwt && !outBwt);
+    const Layout L = planLayout(extentOf(b), io.wantSa && !io.outSa, io.wantBwt && !io.outBwt);
     if (L.peak > c->slabBytes) {
         setError("internal: layout of %llu bytes exceeds the slab of %llu", static_cast<unsigned long long>(L.peak),
                  static_cast<unsigned long long>(c->slabBytes));
         return SADCS_FAILED;
     }
+    const uint64_t launchesBefore = tLaunches;
     uint8_t* slab = c->slab;
     uint8_t* text = slab + L.text;
     uint32_t* ranks = reinterpret_cast<uint32_t*>(slab + L.ranks);
+    uint32_t* meta = reinterpret_cast<uint32_t*>(slab + L.meta);
+    const uint32_t J = b.count;
+    uint32_t* dStart = meta;
+    uint32_t* dEnd = dStart + J;
+    uint32_t* dSampleBase = dEnd + J;
+    uint32_t* dOutBase = dSampleBase + J;
+    uint32_t* dRowZero = dOutBase + J + 1;
+    uint32_t* dClassTables = dRowZero + J;
+    uint32_t* dBlockText = dClassTables + ClassTables::words(J);
+    ClassTables classTables;
+    classTables.carve(dClassTables, J);
     cudaError_t error;
-    auto start = std::chrono::steady_clock::now();
 
-    if ((error = cudaMemsetAsync(text + n, 0, kTextPad, stream)) != cudaSuccess) return failed("upload", error);
-    if (hostText) {
-        s.pinned = isPinned(hostText) ? 1 : 0;
-        if ((error = cudaMemcpyAsync(text, hostText, n, cudaMemcpyHostToDevice, stream)) != cudaSuccess ||
-            (error = cudaStreamSynchronize(stream)) != cudaSuccess) {
+    // The tables, staged in page-locked memory and copied in one piece.
+    uint32_t* h = c->hostWords + 64;
+    std::copy(b.start.begin(), b.start.end(), h);
+    std::copy(b.end.begin(), b.end.end(), h + J);
+    std::copy(b.sampleBase.begin(), b.sampleBase.end(), h + 2 * J);
+    std::copy(b.outBase.begin(), b.outBase.end(), h + 3 * J);
+    std::fill(h + 4 * J + 1, h + 5 * J + 1, 0u);
+    std::copy(b.classTables.begin(), b.classTables.end(), h + 5 * J + 1);
+    if ((error = cudaMemcpyAsync(meta, h, 4 * (5 * static_cast<size_t>(J) + 1 + b.classTables.size()),
+                                 cudaMemcpyHostToDevice, stream)) != cudaSuccess) {
+        return failed("tables", error);
+    }
+
+    TextSet texts{};
+    texts.count = J;
+    texts.start = dStart;
+    texts.end = dEnd;
+    texts.oneEnd = J == 1 ? b.end[0] : 0;
+    texts.blockText = J > 1 ? dBlockText : nullptr;
+
+    // Upload: one text straight into place; several through the ranking region, then placed.
+    auto start = std::chrono::steady_clock::now();
+    const uint8_t* source = io.hostText ? io.hostText : io.deviceText;
+    if (J == 1) {
+        if ((error = cudaMemsetAsync(text + b.end[0], 0, b.span + kTextPad - b.end[0], stream)) != cudaSuccess ||
+            (error = cudaMemcpyAsync(text, source, b.outputs, io.hostText ? cudaMemcpyHostToDevice
+                                                                           : cudaMemcpyDeviceToDevice, stream)) !=
+                cudaSuccess) {
             return failed("upload", error);
         }
+    } else {
+        uint8_t* staging = slab + L.lst0;
+        uint32_t* packedOffset = reinterpret_cast<uint32_t*>(slab + L.classScratch);  // free until the classes
+        if ((error = cudaMemcpyAsync(staging, source, b.outputs,
+                                     io.hostText ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, stream)) !=
+                cudaSuccess ||
+            (error = cudaMemcpyAsync(packedOffset, dOutBase, 4 * static_cast<size_t>(J), cudaMemcpyDeviceToDevice,
+                                     stream)) != cudaSuccess) {
+            return failed("upload", error);
+        }
+        if ((error = launch(placeTexts, J, 256, 0, stream, staging, dStart, dEnd, packedOffset, J,
+                            static_cast<uint32_t>(b.span), text)) != cudaSuccess ||
+            (error = launch(fillBlockText, J, 256, 0, stream, dStart, J, static_cast<uint32_t>(b.span), dBlockText)) !=
+                cudaSuccess) {
+            return failed("placing the texts", error);
+        }
+    }
+    if (io.hostText) {
+        s.pinned = isPinned(io.hostText) ? 1 : 0;
+        if ((error = cudaStreamSynchronize(stream)) != cudaSuccess) return failed("upload", error);
         s.upload_seconds = secondsSince(start);
-    } else if ((error = cudaMemcpyAsync(text, deviceText, n, cudaMemcpyDeviceToDevice, stream)) != cudaSuccess) {
-        return failed("copying the text", error);
     }
     start = std::chrono::steady_clock::now();
     cudaEventRecord(c->events[0], stream);
 
     // Sample ranking.
-    if ((error = cudaMemsetAsync(ranks, 0, 4 * (L.m + kRankPad), stream)) != cudaSuccess) return failed("ranking", error);
+    if (J == 1 && (error = cudaMemsetAsync(ranks, 0, 4 * (b.slots + kRankPad), stream)) != cudaSuccess) {
+        return failed("ranking", error);
+    }
+    if (J > 1 && (error = cudaMemsetAsync(ranks + b.slots, 0, 4 * kRankPad, stream)) != cudaSuccess) {
+        return failed("ranking", error);
+    }
     RankBuffers rb;
     rb.lst[0] = reinterpret_cast<uint32_t*>(slab + L.lst0);
     rb.lst[1] = reinterpret_cast<uint32_t*>(slab + L.lst1);
@@ -282,9 +458,12 @@ int construct(sadcs_gpu_context* c, const uint8_t* hostText, const uint8_t* devi
     rb.aux1 = reinterpret_cast<uint32_t*>(slab + L.aux1);
     rb.aux2 = reinterpret_cast<uint32_t*>(slab + L.aux2);
     rb.scratch = reinterpret_cast<uint32_t*>(slab + L.rankScratch);
+    rb.scanScratch = reinterpret_cast<uint32_t*>(slab + L.scanScratch);
     rb.counter = reinterpret_cast<uint32_t*>(slab + L.counter);
     RankStats rankStats;
-    if ((error = rankSample(text, static_cast<uint32_t>(n), ranks, rb, c->hostWords, stream, rankStats)) != cudaSuccess) {
+    if ((error = rankSample(text, texts, static_cast<uint32_t>(b.slots), static_cast<uint32_t>(b.live), dSampleBase,
+                            static_cast<uint32_t>(b.longest), ranks, rb, c->hostWords, stream, rankStats)) !=
+        cudaSuccess) {
         return failed("sample ranking", error);
     }
     s.character_passes = rankStats.characterPasses;
@@ -297,24 +476,30 @@ int construct(sadcs_gpu_context* c, const uint8_t* hostText, const uint8_t* devi
 
     // Class lists.
     uint32_t* lists = reinterpret_cast<uint32_t*>(slab + L.lists);
-    if ((error = sortClasses(text, static_cast<uint32_t>(n), ranks, lists,
-                             reinterpret_cast<uint32_t*>(slab + L.classScratch), stream)) != cudaSuccess) {
+    uint32_t* classScratch = reinterpret_cast<uint32_t*>(slab + L.classScratch);
+    if ((error = sortClasses(text, J == 1 ? b.end[0] : b.end[J - 1], texts, ranks, static_cast<uint32_t>(b.slots),
+                             b.classes, classTables, lists, classScratch, stream)) != cudaSuccess) {
         return failed("class sorts", error);
     }
     cudaEventRecord(c->events[2], stream);
-    if ((error = cudaStreamSynchronize(stream)) != cudaSuccess) return failed("class sorts", error);
+    if ((error = cudaMemcpyAsync(c->hostWords + 2, classErrorWord(classScratch, J), sizeof(uint32_t),
+                                 cudaMemcpyDeviceToHost, stream)) != cudaSuccess ||
+        (error = cudaStreamSynchronize(stream)) != cudaSuccess) {
+        return failed("class sorts", error);
+    }
+    if (c->hostWords[2]) return failed("class sorts", cudaErrorLaunchTimeout);
     s.class_sort_seconds = secondsSince(start);
     s.class_sort_bytes = static_cast<int64_t>(L.classEnd);
     start = std::chrono::steady_clock::now();
 
     // Merge.
-    uint32_t* sa = outSa ? outSa : (wantSa ? reinterpret_cast<uint32_t*>(slab + L.sa) : nullptr);
-    uint8_t* bwt = outBwt ? outBwt : (wantBwt ? slab + L.bwt : nullptr);
-    if ((error = mergeClasses(text, ranks, static_cast<uint32_t>(n), lists, L.merge,
+    uint32_t* sa = io.outSa ? io.outSa : (io.wantSa ? reinterpret_cast<uint32_t*>(slab + L.sa) : nullptr);
+    uint8_t* bwt = io.outBwt ? io.outBwt : (io.wantBwt ? slab + L.bwt : nullptr);
+    if ((error = mergeClasses(text, ranks, texts, lists, b.merge, classTables.rowBase, dOutBase, dRowZero,
                               reinterpret_cast<uint32_t*>(slab + L.splitters),
                               reinterpret_cast<MergeRow*>(slab + L.rows), sa, bwt,
-                              reinterpret_cast<uint32_t*>(slab + L.mergeCounter), c->hostWords, stream, &row0)) !=
-        cudaSuccess) {
+                              reinterpret_cast<uint32_t*>(slab + L.mergeCounter), c->hostWords, stream,
+                              c->events[4], c->events[5])) != cudaSuccess) {
         return failed("merge", error);
     }
     cudaEventRecord(c->events[3], stream);
@@ -323,14 +508,21 @@ int construct(sadcs_gpu_context* c, const uint8_t* hostText, const uint8_t* devi
     s.merge_bytes = static_cast<int64_t>(L.mergeEnd);
     s.device_bytes = static_cast<int64_t>(L.peak);
     s.device_seconds = elapsedMs(c->events[0], c->events[3]) / 1000.0;
-    internalSa = outSa ? nullptr : sa;
-    internalBwt = outBwt ? nullptr : bwt;
+    s.ranking_device_ms = elapsedMs(c->events[0], c->events[1]);
+    s.class_sort_device_ms = elapsedMs(c->events[1], c->events[2]);
+    s.merge_device_ms = elapsedMs(c->events[2], c->events[3]);
+    s.merge_kernel_ms = elapsedMs(c->events[4], c->events[5]);
+    s.kernel_launches = static_cast<int64_t>(tLaunches - launchesBefore);
+    io.deviceSa = sa;
+    io.deviceBwt = bwt;
+    io.rowZero = dRowZero;
     return SADCS_OK;
 }
 
-// Runs body(context) with the given context, or a temporary one for n bytes (its creation is setup).
+// Runs body(context) with the given context, or a temporary one for `total` bytes in `texts` texts
+// (its creation is setup).
 template <class Body>
-int withContext(sadcs_gpu_context* context, uint64_t n, sadcs_gpu_stats& s, Body body) {
+int withContext(sadcs_gpu_context* context, uint64_t total, uint32_t texts, sadcs_gpu_stats& s, Body body) {
     if (context) {
         int previous = 0;
         cudaGetDevice(&previous);
@@ -341,7 +533,9 @@ int withContext(sadcs_gpu_context* context, uint64_t n, sadcs_gpu_stats& s, Body
     }
     const auto start = std::chrono::steady_clock::now();
     sadcs_gpu_context* temporary = nullptr;
-    if (const int status = createContext(static_cast<int64_t>(n), &temporary); status != SADCS_OK) return status;
+    if (const int status = createContext(static_cast<int64_t>(total), texts, &temporary); status != SADCS_OK) {
+        return status;
+    }
     s.setup_seconds = secondsSince(start);
     const int status = body(temporary);
     const double setup = s.setup_seconds;
@@ -351,6 +545,7 @@ int withContext(sadcs_gpu_context* context, uint64_t n, sadcs_gpu_stats& s, Body
 }
 
 int download(sadcs_gpu_context* c, void* host, const void* device, size_t bytes, sadcs_gpu_stats& s) {
+    if (bytes == 0) return SADCS_OK;
     const auto start = std::chrono::steady_clock::now();
     cudaError_t error;
     if ((error = cudaMemcpyAsync(host, device, bytes, cudaMemcpyDeviceToHost, c->stream)) != cudaSuccess ||
@@ -358,6 +553,43 @@ int download(sadcs_gpu_context* c, void* host, const void* device, size_t bytes,
         return failed("download", error);
     }
     s.download_seconds += secondsSince(start);
+    return SADCS_OK;
+}
+
+// The rows of the texts' first suffixes, read back: primary = row + 1 per text.
+int readPrimaries(sadcs_gpu_context* c, const Io& io, uint32_t count, int64_t* primaries) {
+    uint32_t* h = c->hostWords + 64;
+    cudaError_t error;
+    if ((error = cudaMemcpyAsync(h, io.rowZero, 4 * static_cast<size_t>(count), cudaMemcpyDeviceToHost, c->stream)) !=
+            cudaSuccess ||
+        (error = cudaStreamSynchronize(c->stream)) != cudaSuccess) {
+        return failed("download", error);
+    }
+    for (uint32_t j = 0; j < count; j++) primaries[j] = static_cast<int64_t>(h[j]) + 1;
+    return SADCS_OK;
+}
+
+// A batch of the non-empty texts among lengths[0, count): their indices in `kept`.
+int batchOf(const int64_t* lengths, int64_t count, Batch& b, std::vector<uint32_t>& kept) {
+    if (count < 0 || count > static_cast<int64_t>(kMaxTexts)) {
+        setError("%lld texts out of range (at most %u)", static_cast<long long>(count), kMaxTexts);
+        return SADCS_FAILED;
+    }
+    std::vector<uint64_t> nonEmpty;
+    for (int64_t j = 0; j < count; j++) {
+        if (lengths[j] < 0) {
+            setError("text %lld has a negative length", static_cast<long long>(j));
+            return SADCS_FAILED;
+        }
+        if (lengths[j] > 0) {
+            nonEmpty.push_back(static_cast<uint64_t>(lengths[j]));
+            kept.push_back(static_cast<uint32_t>(j));
+        }
+    }
+    if (!planBatch(nonEmpty.data(), static_cast<uint32_t>(nonEmpty.size()), b)) {
+        setError("texts exceed %lld bytes together", static_cast<long long>(kMaxText));
+        return SADCS_FAILED;
+    }
     return SADCS_OK;
 }
 
@@ -380,7 +612,12 @@ int sadcs_gpu_query_device(sadcs_gpu_device* device) {
 
 int64_t sadcs_gpu_required_bytes(int64_t n) {
     if (n < 0 || n > kMaxText) return -1;
-    return n == 0 ? 0 : static_cast<int64_t>(planLayout(static_cast<uint64_t>(n), true, true).peak);
+    return n == 0 ? 0 : static_cast<int64_t>(contextBytes(n, 1));
+}
+
+int64_t sadcs_gpu_required_bytes_batch(int64_t total, int64_t texts) {
+    if (total < 0 || total > kMaxText || texts < 1 || texts > static_cast<int64_t>(kMaxTexts)) return -1;
+    return static_cast<int64_t>(contextBytes(total, static_cast<uint32_t>(texts)));
 }
 
 int sadcs_gpu_create_context(int64_t capacity, sadcs_gpu_context** context) {
@@ -389,7 +626,20 @@ int sadcs_gpu_create_context(int64_t capacity, sadcs_gpu_context** context) {
         setError("context pointer is null");
         return SADCS_FAILED;
     }
-    return createContext(std::max<int64_t>(capacity, 0), context);
+    return createContext(std::max<int64_t>(capacity, 0), 1, context);
+}
+
+int sadcs_gpu_create_batch_context(int64_t capacity, int64_t max_texts, sadcs_gpu_context** context) {
+    tLastError[0] = '\0';
+    if (!context) {
+        setError("context pointer is null");
+        return SADCS_FAILED;
+    }
+    if (max_texts < 1 || max_texts > static_cast<int64_t>(kMaxTexts)) {
+        setError("max_texts %lld out of range (1 to %u)", static_cast<long long>(max_texts), kMaxTexts);
+        return SADCS_FAILED;
+    }
+    return createContext(std::max<int64_t>(capacity, 0), static_cast<uint32_t>(max_texts), context);
 }
 
 void sadcs_gpu_destroy_context(sadcs_gpu_context* context) {
@@ -400,38 +650,105 @@ int64_t sadcs_gpu_context_capacity(const sadcs_gpu_context* context) {
     return context ? static_cast<int64_t>(context->capacity) : 0;
 }
 
-int sadcs_gpu_build(sadcs_gpu_context* context, const uint8_t* text, int64_t n, uint32_t* sa, uint8_t* bwt,
-                    int64_t* primary, sadcs_gpu_stats* stats) {
+int sadcs_gpu_build_batch(sadcs_gpu_context* context, const uint8_t* texts, const int64_t* lengths, int64_t count,
+                          uint32_t* sa, uint8_t* bwt, int64_t* primaries, sadcs_gpu_stats* stats) {
     tLastError[0] = '\0';
     sadcs_gpu_stats local{};
     sadcs_gpu_stats& s = stats ? *stats : local;
     s = sadcs_gpu_stats{};
-    if (primary) *primary = n > 0 ? -1 : 0;
     if (!sa && !bwt) {
         setError("neither a suffix array nor a BWT was asked for");
         return SADCS_FAILED;
     }
-    if (n > kMaxText) {
-        setError("text of %lld bytes exceeds the limit of %lld", static_cast<long long>(n), static_cast<long long>(kMaxText));
+    if (count > 0 && !lengths) {
+        setError("lengths is null");
         return SADCS_FAILED;
     }
-    if (n <= 0) return context ? SADCS_OK : queryDevice(nullptr);
-    if (!text) {
-        setError("text is null");
+    for (int64_t j = 0; primaries && j < count; j++) primaries[j] = 0;
+    Batch b;
+    std::vector<uint32_t> kept;
+    if (const int status = batchOf(lengths, count, b, kept); status != SADCS_OK) return status;
+    if (b.count == 0) return context ? SADCS_OK : queryDevice(nullptr);
+    if (!texts) {
+        setError("texts is null");
         return SADCS_FAILED;
     }
-    return withContext(context, static_cast<uint64_t>(n), s, [&](sadcs_gpu_context* c) -> int {
-        uint32_t* deviceSa = nullptr;
-        uint8_t* deviceBwt = nullptr;
-        uint32_t row0 = 0;
-        int status = construct(c, text, nullptr, static_cast<uint64_t>(n), sa != nullptr, bwt != nullptr, nullptr,
-                               nullptr, c->stream, s, deviceSa, deviceBwt, row0);
+    return withContext(context, b.outputs, b.count, s, [&](sadcs_gpu_context* c) -> int {
+        Io io;
+        io.hostText = texts;
+        io.wantSa = sa != nullptr;
+        io.wantBwt = bwt != nullptr;
+        int status = construct(c, b, io, c->stream, s);
         if (status != SADCS_OK) return status;
-        if (sa && (status = download(c, sa, deviceSa, 4 * static_cast<size_t>(n), s)) != SADCS_OK) return status;
-        if (bwt && (status = download(c, bwt, deviceBwt, static_cast<size_t>(n), s)) != SADCS_OK) return status;
-        if (primary) *primary = bwt ? static_cast<int64_t>(row0) + 1 : -1;
+        if (sa && (status = download(c, sa, io.deviceSa, 4 * b.outputs, s)) != SADCS_OK) return status;
+        if (bwt && (status = download(c, bwt, io.deviceBwt, b.outputs, s)) != SADCS_OK) return status;
+        if (bwt && primaries) {
+            std::vector<int64_t> p(b.count);
+            if ((status = readPrimaries(c, io, b.count, p.data())) != SADCS_OK) return status;
+            for (uint32_t k = 0; k < b.count; k++) primaries[kept[k]] = p[k];
+        }
         return SADCS_OK;
     });
+}
+
+int sadcs_gpu_build_batch_device(sadcs_gpu_context* context, const uint8_t* d_texts, const int64_t* lengths,
+                                 int64_t count, uint32_t* d_sa, uint8_t* d_bwt, int64_t* primaries, void* stream,
+                                 sadcs_gpu_stats* stats) {
+    tLastError[0] = '\0';
+    sadcs_gpu_stats local{};
+    sadcs_gpu_stats& s = stats ? *stats : local;
+    s = sadcs_gpu_stats{};
+    if (!d_sa && !d_bwt) {
+        setError("neither a suffix array nor a BWT was asked for");
+        return SADCS_FAILED;
+    }
+    if (count > 0 && !lengths) {
+        setError("lengths is null");
+        return SADCS_FAILED;
+    }
+    for (int64_t j = 0; primaries && j < count; j++) primaries[j] = 0;
+    Batch b;
+    std::vector<uint32_t> kept;
+    if (const int status = batchOf(lengths, count, b, kept); status != SADCS_OK) return status;
+    if (b.count == 0) return context ? SADCS_OK : queryDevice(nullptr);
+    return withContext(context, b.outputs, b.count, s, [&](sadcs_gpu_context* c) -> int {
+        Io io;
+        io.deviceText = d_texts;
+        io.wantSa = d_sa != nullptr;
+        io.wantBwt = d_bwt != nullptr;
+        io.outSa = d_sa;
+        io.outBwt = d_bwt;
+        cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : c->stream;
+        const int status = construct(c, b, io, st, s);
+        if (status != SADCS_OK) return status;
+        if (d_bwt && primaries) {
+            uint32_t* h = c->hostWords + 64;
+            cudaError_t error;
+            if ((error = cudaMemcpyAsync(h, io.rowZero, 4 * static_cast<size_t>(b.count), cudaMemcpyDeviceToHost, st)) !=
+                    cudaSuccess ||
+                (error = cudaStreamSynchronize(st)) != cudaSuccess) {
+                return failed("download", error);
+            }
+            for (uint32_t k = 0; k < b.count; k++) primaries[kept[k]] = static_cast<int64_t>(h[k]) + 1;
+        }
+        return SADCS_OK;
+    });
+}
+
+int sadcs_gpu_build(sadcs_gpu_context* context, const uint8_t* text, int64_t n, uint32_t* sa, uint8_t* bwt,
+                    int64_t* primary, sadcs_gpu_stats* stats) {
+    if (n > kMaxText) {
+        tLastError[0] = '\0';
+        setError("text of %lld bytes exceeds the limit of %lld", static_cast<long long>(n), static_cast<long long>(kMaxText));
+        if (stats) *stats = sadcs_gpu_stats{};
+        return SADCS_FAILED;
+    }
+    const int64_t length = std::max<int64_t>(n, 0);
+    int64_t p = 0;
+    const int status = sadcs_gpu_build_batch(context, text, &length, 1, sa, bwt, &p, stats);
+    if (primary) *primary = status == SADCS_OK ? (bwt ? p : -1) : (n > 0 ? -1 : 0);
+    if (primary && n <= 0) *primary = 0;
+    return status;
 }
 
 int sadcs_gpu_suffix_array(sadcs_gpu_context* context, const uint8_t* text, int64_t n, int32_t* sa,
@@ -483,30 +800,17 @@ int sadcs_gpu_bwt(sadcs_gpu_context* context, const uint8_t* text, int64_t n, ui
 
 int sadcs_gpu_build_device(sadcs_gpu_context* context, const uint8_t* d_text, int64_t n, uint32_t* d_sa,
                            uint8_t* d_bwt, int64_t* primary, void* stream, sadcs_gpu_stats* stats) {
-    tLastError[0] = '\0';
-    sadcs_gpu_stats local{};
-    sadcs_gpu_stats& s = stats ? *stats : local;
-    s = sadcs_gpu_stats{};
-    if (primary) *primary = n > 0 ? -1 : 0;
-    if (!d_sa && !d_bwt) {
-        setError("neither a suffix array nor a BWT was asked for");
-        return SADCS_FAILED;
-    }
     if (n > kMaxText) {
+        tLastError[0] = '\0';
         setError("text of %lld bytes exceeds the limit of %lld", static_cast<long long>(n), static_cast<long long>(kMaxText));
+        if (stats) *stats = sadcs_gpu_stats{};
         return SADCS_FAILED;
     }
-    if (n <= 0) return context ? SADCS_OK : queryDevice(nullptr);
-    return withContext(context, static_cast<uint64_t>(n), s, [&](sadcs_gpu_context* c) -> int {
-        uint32_t* unusedSa = nullptr;
-        uint8_t* unusedBwt = nullptr;
-        uint32_t row0 = 0;
-        cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : c->stream;
-        const int status = construct(c, nullptr, d_text, static_cast<uint64_t>(n), d_sa != nullptr, d_bwt != nullptr,
-                                     d_sa, d_bwt, st, s, unusedSa, unusedBwt, row0);
-        if (status == SADCS_OK && primary) *primary = d_bwt ? static_cast<int64_t>(row0) + 1 : -1;
-        return status;
-    });
+    const int64_t length = std::max<int64_t>(n, 0);
+    int64_t p = 0;
+    const int status = sadcs_gpu_build_batch_device(context, d_text, &length, 1, d_sa, d_bwt, &p, stream, stats);
+    if (primary) *primary = n <= 0 ? 0 : (status == SADCS_OK && d_bwt ? p : -1);
+    return status;
 }
 
 int sadcs_gpu_bwt_from_sa(const uint8_t* d_text, int64_t n, const uint32_t* d_sa, uint8_t* d_bwt, int64_t* primary,
@@ -537,6 +841,64 @@ int sadcs_gpu_bwt_from_sa(const uint8_t* d_text, int64_t n, const uint32_t* d_sa
     return SADCS_OK;
 }
 
+int sadcs_gpu_check_suffix_array(const uint8_t* d_text, int64_t n, const uint32_t* d_sa, int64_t* bad_index,
+                                 const char** reason, void* stream) {
+    tLastError[0] = '\0';
+    if (bad_index) *bad_index = -1;
+    if (reason) *reason = nullptr;
+    if (n <= 0) return SADCS_OK;
+    if (n > kMaxText) {
+        setError("text of %lld bytes exceeds the limit of %lld", static_cast<long long>(n), static_cast<long long>(kMaxText));
+        return SADCS_FAILED;
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const uint32_t count = static_cast<uint32_t>(n);
+    uint32_t* isa = nullptr;
+    unsigned long long* words = nullptr;
+    unsigned long long* host = nullptr;
+    cudaError_t error;
+    if ((error = cudaMallocAsync(&isa, 4 * static_cast<size_t>(n), st)) != cudaSuccess) return failed("cudaMallocAsync", error);
+    if ((error = cudaMallocAsync(&words, 3 * sizeof(unsigned long long), st)) != cudaSuccess ||
+        (error = cudaMallocHost(&host, 3 * sizeof(unsigned long long))) != cudaSuccess) {
+        cudaFreeAsync(isa, st);
+        if (words) cudaFreeAsync(words, st);
+        return failed("allocating check buffers", error);
+    }
+    const uint32_t blocks = (count + 255) / 256;
+    error = cudaMemsetAsync(words, 0xFF, 3 * sizeof(unsigned long long), st);
+    if (error == cudaSuccess) error = launch(checkScatter, blocks, 256, 0, st, d_sa, count, isa, words);
+    if (error == cudaSuccess) error = cudaMemcpyAsync(host, words, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
+    if (error == cudaSuccess) error = cudaStreamSynchronize(st);
+    const char* why = nullptr;
+    int64_t index = -1;
+    if (error == cudaSuccess && host[0] != kNoFailure) {
+        why = "entry out of range";
+        index = static_cast<int64_t>(host[0]);
+    }
+    if (error == cudaSuccess && !why) {
+        error = launch(checkDuplicates, blocks, 256, 0, st, d_sa, count, isa, words + 1);
+        if (error == cudaSuccess) error = launch(checkOrder, blocks, 256, 0, st, d_text, d_sa, count, isa, words + 2);
+        if (error == cudaSuccess)
+            error = cudaMemcpyAsync(host + 1, words + 1, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
+        if (error == cudaSuccess) error = cudaStreamSynchronize(st);
+        if (error == cudaSuccess && host[1] != kNoFailure) {
+            why = "duplicate entry";
+            index = static_cast<int64_t>(host[1]);
+        } else if (error == cudaSuccess && host[2] != kNoFailure) {
+            why = "SA[index] and SA[index + 1] out of order";
+            index = static_cast<int64_t>(host[2]);
+        }
+    }
+    cudaFreeAsync(isa, st);
+    cudaFreeAsync(words, st);
+    cudaStreamSynchronize(st);
+    cudaFreeHost(host);
+    if (error != cudaSuccess) return failed("suffix array check", error);
+    if (bad_index) *bad_index = index;
+    if (reason) *reason = why;
+    return SADCS_OK;
+}
+
 int sadcs_gpu_rank_sample(const uint8_t* text, int64_t n, uint32_t* ranks, sadcs_gpu_stats* stats) {
     tLastError[0] = '\0';
     sadcs_gpu_stats local{};
@@ -547,16 +909,18 @@ int sadcs_gpu_rank_sample(const uint8_t* text, int64_t n, uint32_t* ranks, sadcs
         setError("text of %lld bytes exceeds the limit of %lld", static_cast<long long>(n), static_cast<long long>(kMaxText));
         return SADCS_FAILED;
     }
-    return withContext(nullptr, static_cast<uint64_t>(n), s, [&](sadcs_gpu_context* c) -> int {
-        const Layout L = planLayout(static_cast<uint64_t>(n), false, false);
+    const uint64_t length = static_cast<uint64_t>(n);
+    Batch b;
+    planBatch(&length, 1, b);
+    return withContext(nullptr, length, 1, s, [&](sadcs_gpu_context* c) -> int {
+        const Layout L = planLayout(extentOf(b), false, false);
         uint8_t* textBuffer = c->slab + L.text;
         uint32_t* rankBuffer = reinterpret_cast<uint32_t*>(c->slab + L.ranks);
         cudaError_t error;
         auto start = std::chrono::steady_clock::now();
-        if ((error = cudaMemsetAsync(textBuffer + n, 0, kTextPad, c->stream)) != cudaSuccess ||
-            (error = cudaMemcpyAsync(textBuffer, text, static_cast<size_t>(n), cudaMemcpyHostToDevice, c->stream)) !=
-                cudaSuccess ||
-            (error = cudaMemsetAsync(rankBuffer, 0, 4 * (L.m + kRankPad), c->stream)) != cudaSuccess ||
+        if ((error = cudaMemsetAsync(textBuffer + n, 0, b.span + kTextPad - length, c->stream)) != cudaSuccess ||
+            (error = cudaMemcpyAsync(textBuffer, text, length, cudaMemcpyHostToDevice, c->stream)) != cudaSuccess ||
+            (error = cudaMemsetAsync(rankBuffer, 0, 4 * (b.slots + kRankPad), c->stream)) != cudaSuccess ||
             (error = cudaStreamSynchronize(c->stream)) != cudaSuccess) {
             return failed("upload", error);
         }
@@ -571,9 +935,14 @@ int sadcs_gpu_rank_sample(const uint8_t* text, int64_t n, uint32_t* ranks, sadcs
         rb.aux1 = reinterpret_cast<uint32_t*>(c->slab + L.aux1);
         rb.aux2 = reinterpret_cast<uint32_t*>(c->slab + L.aux2);
         rb.scratch = reinterpret_cast<uint32_t*>(c->slab + L.rankScratch);
+        rb.scanScratch = reinterpret_cast<uint32_t*>(c->slab + L.scanScratch);
         rb.counter = reinterpret_cast<uint32_t*>(c->slab + L.counter);
+        TextSet texts{};
+        texts.count = 1;
+        texts.oneEnd = static_cast<uint32_t>(length);
         RankStats rankStats;
-        if ((error = rankSample(textBuffer, static_cast<uint32_t>(n), rankBuffer, rb, c->hostWords, c->stream,
+        if ((error = rankSample(textBuffer, texts, static_cast<uint32_t>(b.slots), static_cast<uint32_t>(b.live),
+                                nullptr, static_cast<uint32_t>(length), rankBuffer, rb, c->hostWords, c->stream,
                                 rankStats)) != cudaSuccess) {
             return failed("sample ranking", error);
         }
@@ -583,7 +952,7 @@ int sadcs_gpu_rank_sample(const uint8_t* text, int64_t n, uint32_t* ranks, sadcs
         s.device_seconds = s.ranking_seconds;
         s.ranking_bytes = static_cast<int64_t>(L.rankingEnd);
         s.device_bytes = s.ranking_bytes;
-        return download(c, ranks, rankBuffer, 4 * L.m, s);
+        return download(c, ranks, rankBuffer, 4 * b.live, s);
     });
 }
 
@@ -605,3 +974,5 @@ const char* sadcs_gpu_last_error(void) {
 }
 
 }  // extern "C"
+
+#include "server.cuh"

@@ -113,14 +113,11 @@ def natural_text(n: int = 256 << 20, seed: int = 2, vocabulary: int = 50_000, zi
         words = np.minimum(np.searchsorted(cdf, rng.random(count)), vocabulary - 1)
         wl = lengths[words]
         # Sentence ends: ".\n" after every U[10,30] words, a space otherwise.
-        gaps = []
-        pos = until_stop - 1
-        while pos < count:
-            gaps.append(pos)
-            pos += int(rng.integers(10, 31))
-        until_stop = pos - count + 1
+        ends = until_stop - 1 + np.concatenate([[0], np.cumsum(rng.integers(10, 31, count // 10 + 2))])
+        inside = ends[ends < count]
+        until_stop = int(ends[len(inside)]) - count + 1
         stop = np.zeros(count, bool)
-        stop[np.array(gaps, dtype=np.int64)] = True
+        stop[inside] = True
         sep_len = np.where(stop, 2, 1)
         total = wl + sep_len
         offs = np.concatenate([[0], np.cumsum(total)[:-1]])

@@ -157,3 +157,87 @@ def test_device_resident_and_gather():
     p2 = sa.bwt_from_sa_device(d_text.data_ptr(), n, d_sa.data_ptr(), d_bwt2.data_ptr(), stream=stream)
     torch.cuda.synchronize()
     assert p2 == ep and np.array_equal(d_bwt2.cpu().numpy(), eb)
+
+
+def _expected(text):
+    sa_ = oracle.doubling_sa(text)
+    b, p = oracle.bwt_from_sa(text, sa_)
+    return sa_, b, p
+
+
+def test_batch_matches_single_texts():
+    """One construction of many uneven texts: every text's SA and BWT bit-exact with its own."""
+    rng = W.SplitMix(41)
+    texts = [np.frombuffer(b"banana", np.uint8), np.zeros(0, np.uint8), np.frombuffer(b"a", np.uint8),
+             W.run_text(100), W.fibonacci_text(3000), W.periodic_text(rng, 5000, 33), np.zeros(700, np.uint8)]
+    for i in range(40):
+        n = 1 + int(rng.below(6000)[0])
+        texts.append(W.random_text(rng, n, [1, 2, 4, 26, 256][i % 5]))
+    texts += W.batch_texts(24, lo=1 << 10, hi=1 << 17, seed=8)
+    sas, bwts, primaries = sa.build_batch(texts)
+    for j, t in enumerate(texts):
+        es, eb, ep = _expected(t)
+        assert np.array_equal(sas[j], es), f"text {j} (n={len(t)}): SA differs"
+        assert np.array_equal(bwts[j], eb) and primaries[j] == ep, f"text {j} (n={len(t)}): BWT differs"
+
+
+def test_batch_context_reuse_and_device_path():
+    import torch
+
+    texts = W.batch_texts(64, lo=1 << 10, hi=1 << 16, seed=9)
+    lengths = [len(t) for t in texts]
+    total = sum(lengths)
+    with sa.Context(total, max_texts=64) as ctx:
+        for _ in range(2):
+            sas, bwts, primaries = sa.build_batch(texts, context=ctx)
+            for j, t in enumerate(texts):
+                es, eb, ep = _expected(t)
+                assert np.array_equal(sas[j], es) and np.array_equal(bwts[j], eb) and primaries[j] == ep
+        packed = torch.from_numpy(np.concatenate(texts)).cuda()
+        d_sa = torch.empty(total, dtype=torch.int32, device="cuda")
+        d_bwt = torch.empty(total, dtype=torch.uint8, device="cuda")
+        prim = sa.build_batch_device(packed.data_ptr(), lengths, d_sa.data_ptr(), d_bwt.data_ptr(), context=ctx,
+                                     stream=torch.cuda.current_stream().cuda_stream)
+        torch.cuda.synchronize()
+        all_sa = d_sa.cpu().numpy().view(np.uint32)
+        all_bwt = d_bwt.cpu().numpy()
+        off = np.concatenate([[0], np.cumsum(lengths)])
+        for j, t in enumerate(texts):
+            es, eb, ep = _expected(t)
+            assert np.array_equal(all_sa[off[j]:off[j + 1]], es) and np.array_equal(all_bwt[off[j]:off[j + 1]], eb)
+            assert prim[j] == ep
+        with pytest.raises(sa.GpuError) as err:
+            sa.build_batch(texts + [W.run_text(10)], context=ctx)
+        assert err.value.status == sa.GpuStatus.NotEnoughMemory
+
+
+def test_server_results_equal_alone_and_in_the_mix():
+    """Continuous batching: requests submitted while others run; each result equals its own build."""
+    import threading
+    import time
+
+    rng = np.random.default_rng(12)
+    texts = W.batch_texts(60, lo=1 << 10, hi=1 << 18, seed=12) + [W.natural_text(3 << 20, seed=13),
+                                                                 W.run_text(5000), np.zeros(0, np.uint8)]
+    order = rng.permutation(len(texts))
+    with sa.Server(workers=3, small_limit=1 << 20, batch_bytes=16 << 20, batch_texts=64) as server:
+        tickets = {}
+
+        def producer():
+            for k in order:
+                tickets[int(k)] = server.submit(texts[int(k)])
+                time.sleep(0.001)
+
+        thread = threading.Thread(target=producer)
+        thread.start()
+        thread.join()
+        batched = 0
+        for k, ticket in tickets.items():
+            s_, b_, p_, latency, size = server.wait(ticket)
+            es, eb, ep = _expected(texts[k])
+            assert np.array_equal(s_, es) and np.array_equal(b_, eb) and p_ == ep, f"request {k} differs"
+            assert latency[2] >= latency[1] >= 0
+            batched += size > 1
+        assert batched > 0  # some requests shared a construction
+        constructions, launches = server.counters()
+        assert 0 < constructions < len(texts) and launches > 0
