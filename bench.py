@@ -43,6 +43,11 @@ PIPELINE_BYTES_PER_INPUT_BYTE = 82.125
 MERGE_BYTES_PER_INPUT_BYTE = 53.0
 FALLBACK_HBM_GBS = 6650.0
 
+BATCH_DESC = ("4096 texts, lengths log-uniform in [1 KiB, 4 MiB], thirds over {A,C,G,T}, a 20-letter protein-like "
+              "alphabet with background frequencies, and uniform bytes; seed 4; one batched construction per step")
+SERVE_DESC = ("serving stream: Poisson arrivals at offered loads 50/200/800 req/s, lengths log-uniform in "
+              "[4 KiB, 64 MiB] plus 1% at 1 GiB, alphabets as the batched config; seed 5")
+
 WORKLOADS = {
     "natural256m": ("256 MiB natural-language-like text: 50k-word lowercase vocabulary (lengths 2-12), "
                     "Zipf(1.1) words, '.\\n' every 10-30 words, 2% capitalised, seed 2",
@@ -418,13 +423,182 @@ def profile_traffic(workload: str):
         return None
 
 
+def run_batch(args, world, rank, local) -> None:
+    """Config 4: many uneven texts in one construction, against one construction per text."""
+    import torch
+
+    import sadcs_b200 as sa
+    from sadcs_b200 import workloads as W
+
+    torch.cuda.set_device(local)
+    texts = W.batch_texts(args.batch_count, lo=1 << 10, hi=4 << 20, seed=4 + rank)
+    lengths = [len(t) for t in texts]
+    total = sum(lengths)
+    packed = torch.from_numpy(np.concatenate(texts)).to(f"cuda:{local}")
+    d_sa = torch.empty(total, dtype=torch.int32, device=f"cuda:{local}")
+    d_bwt = torch.empty(total, dtype=torch.uint8, device=f"cuda:{local}")
+    ctx = sa.Context(total, max_texts=len(texts))
+    stream = torch.cuda.current_stream()
+    stats = sa.Stats()
+
+    def step():
+        return sa.build_batch_device(packed.data_ptr(), lengths, d_sa.data_ptr(), d_bwt.data_ptr(), context=ctx,
+                                     stream=stream.cuda_stream, stats=stats)
+
+    for _ in range(max(args.warmup, 0)):
+        step()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(None)
+    sampler.start()
+    barrier(world)
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches = 0
+    start.record(stream)
+    for _ in range(args.steps):
+        step()
+        launches += int(stats.kernel_launches)
+    stop.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    clocks = sampler.stop()
+    ms = start.elapsed_time(stop) / args.steps
+    ms_max = max_over_ranks(ms, world)
+    value = sum_over_ranks(float(total), world) / MIB / (ms_max / 1e3)
+
+    # The plain path: one construction per text (a bounded sample of the same texts), device-resident.
+    sample = texts[:: max(1, len(texts) // args.plain_sample)][: args.plain_sample]
+    one = sa.Context(max(len(t) for t in sample))
+    plain_bytes, plain_ms = 0, 0.0
+    for t in sample:
+        d_t = torch.from_numpy(t).to(f"cuda:{local}")
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        sa.build_device(d_t.data_ptr(), len(t), d_sa.data_ptr(), d_bwt.data_ptr(), context=one,
+                        stream=stream.cuda_stream)
+        b.record(stream)
+        torch.cuda.synchronize()
+        plain_ms += a.elapsed_time(b)
+        plain_bytes += len(t)
+    one.close()
+    plain = plain_bytes / MIB / (plain_ms / 1e3)
+    if rank == 0:
+        print(json.dumps({
+            "metric": "batched input MB/s (bit-exact SA+BWT per text)", "value": round(value, 3), "unit": UNIT,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_max, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+            "config": {"workload": "batch4096", "description": BATCH_DESC, "texts": len(texts), "total_bytes": total,
+                       "l2": "inputs larger than L2", "parallelism": "independent batches per GPU"},
+            "texts_per_s": round(len(texts) * world / (ms_max / 1e3), 1),
+            "plain_one_text_per_launch": {"value": round(plain, 3), "unit": UNIT, "texts": len(sample),
+                                          "texts_per_s": round(len(sample) / (plain_ms / 1e3), 1)},
+            "speedup_vs_plain": round(value / world / plain, 2), "clocks": clocks, "gpu_launches": launches,
+        }), flush=True)
+
+
+def run_serve(args, world, rank, local) -> None:
+    """Config 5: Poisson request streams through the server; p50/p99 latency at each offered load."""
+    import threading
+
+    import torch
+
+    import sadcs_b200 as sa
+
+    torch.cuda.set_device(local)
+    rng = np.random.default_rng(5 + rank)
+    loads = [float(x) for x in args.serve_loads.split(",")]
+    results = []
+    for load in loads:
+        count = args.serve_requests
+        lengths = np.exp(rng.uniform(np.log(4 << 10), np.log(64 << 20), count)).astype(np.int64)
+        huge = rng.random(count) < args.serve_huge_fraction
+        lengths[huge] = 1 << 30
+        kinds = rng.integers(0, 3, count)
+        pool = {}
+
+        def text_of(i):
+            n = int(lengths[i])
+            key = (n, int(kinds[i]))
+            if key not in pool:
+                g = np.random.default_rng(n * 3 + int(kinds[i]))
+                if kinds[i] == 0:
+                    pool[key] = np.frombuffer(b"ACGT", np.uint8)[g.integers(0, 4, n)]
+                elif kinds[i] == 1:
+                    from sadcs_b200.workloads import protein_text
+                    pool[key] = protein_text(g, n)
+                else:
+                    pool[key] = g.integers(0, 256, n, dtype=np.uint8)
+            return pool[key]
+
+        texts = [text_of(i) for i in range(count)]
+        arrivals = np.cumsum(rng.exponential(1.0 / load, count))
+        server = sa.Server(workers=args.serve_workers, small_limit=4 << 20, batch_bytes=256 << 20,
+                           batch_texts=4096)
+        tickets = [None] * count
+        t0 = time.perf_counter()
+
+        def producer():
+            for i in range(count):
+                delay = arrivals[i] - (time.perf_counter() - t0)
+                if delay > 0:
+                    time.sleep(delay)
+                tickets[i] = server.submit(texts[i])
+
+        thread = threading.Thread(target=producer)
+        thread.start()
+        thread.join()
+        latencies, batch_sizes = [], []
+        for i in range(count):
+            _, _, _, lat, size = server.wait(tickets[i])
+            latencies.append(lat[2])
+            batch_sizes.append(size)
+        elapsed = time.perf_counter() - t0
+        constructions, launches = server.counters()
+        server.close()
+        total_bytes = float(lengths.sum())
+        results.append({"offered_req_s": load, "requests": count, "req_s": round(count / elapsed, 2),
+                        "mib_s": round(total_bytes / MIB / elapsed, 2),
+                        "p50_ms": round(float(np.percentile(latencies, 50)) * 1e3, 2),
+                        "p99_ms": round(float(np.percentile(latencies, 99)) * 1e3, 2),
+                        "mean_batch": round(float(np.mean(batch_sizes)), 2), "constructions": constructions,
+                        "gpu_launches": launches})
+    # One-at-a-time plain construction on a sample of the same request shapes.
+    ctx = sa.Context(64 << 20)
+    plain_bytes, plain_s = 0, 0.0
+    g = np.random.default_rng(99)
+    for n in np.exp(g.uniform(np.log(4 << 10), np.log(64 << 20), args.plain_sample)).astype(np.int64):
+        t = g.integers(0, 256, int(n), dtype=np.uint8)
+        a = time.perf_counter()
+        sa.build(t, context=ctx)
+        plain_s += time.perf_counter() - a
+        plain_bytes += int(n)
+    ctx.close()
+    if rank == 0:
+        best = max(results, key=lambda r: r["mib_s"])
+        print(json.dumps({
+            "metric": "served input MB/s with p50/p99 latency (bit-exact SA+BWT)", "value": best["mib_s"],
+            "unit": UNIT, "n_gpus": world, "steps": len(loads), "warmup": 0, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+            "config": {"workload": "serve", "description": SERVE_DESC, "workers": args.serve_workers},
+            "loads": results,
+            "plain_one_at_a_time": {"value": round(plain_bytes / MIB / plain_s, 2), "unit": UNIT,
+                                    "requests": args.plain_sample, "api": "sadcs_gpu_build, host to host"},
+        }), flush=True)
+
+
 def main() -> None:
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--workload", choices=sorted(WORKLOADS), default="natural256m")
+    p.add_argument("--workload", choices=sorted(WORKLOADS) + ["batch4096", "serve"], default="natural256m")
+    p.add_argument("--batch-count", type=int, default=4096)
+    p.add_argument("--plain-sample", type=int, default=64)
+    p.add_argument("--serve-loads", default="50,200,800")
+    p.add_argument("--serve-requests", type=int, default=200)
+    p.add_argument("--serve-huge-fraction", type=float, default=0.01)
+    p.add_argument("--serve-workers", type=int, default=3)
     p.add_argument("--cpu-sample-mib", type=int, default=64)
     p.add_argument("--reference-sample-mib", type=int, default=64)
     p.add_argument("--e2e-steps", type=int, default=3)
@@ -434,7 +608,16 @@ def main() -> None:
     world, rank, local = dist_setup(args.gpus)
     try:
         if args.impl == "reference":
-            run_reference(args, world, rank)
+            if args.workload in ("batch4096", "serve"):
+                if rank == 0:
+                    print(json.dumps({"impl": "reference", "unavailable": "the reference has no batched or served "
+                                      "construction (one text per call); its per-text CPU rate is the natural256m line"}))
+            else:
+                run_reference(args, world, rank)
+        elif args.workload == "batch4096":
+            run_batch(args, world, rank, local)
+        elif args.workload == "serve":
+            run_serve(args, world, rank, local)
         else:
             run_ours(args, world, rank, local)
     finally:

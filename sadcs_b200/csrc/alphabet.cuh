@@ -1,0 +1,107 @@
+// alphabet.cuh - the texts' alphabet and the packed code stream the ranking keys and the merge
+// records are cut from.
+//
+// Every byte value present in the texts gets a code, in byte order (so code order is byte order),
+// of b = bit_width(sigma - 1) bits (at least 1). The codes of the concatenation are packed into a
+// big-endian bit stream of 64-bit words: character q occupies bits [q*b, (q+1)*b) counted from the
+// most significant bit of word 0, so 64 bits taken at bit q*b hold characters q, q+1, ... with
+// character q on top and compare as integers exactly as the byte strings compare. Positions past a
+// text's end read code 0 (the smallest character): a shorter suffix can tie with a longer one there
+// but never sort after it, and the length tags and text ends separate them (as zero padding does
+// for bytes). DNA packs 29 characters into a ranking key (bytes: 7) and 64 into a merge record's 16
+// bytes (bytes: 16).
+#pragma once
+
+#include "common.cuh"
+
+namespace sadcs {
+
+struct CodeTable {
+    uint8_t code[256];
+};
+
+// counts[c] += occurrences of byte c inside the texts (zeroed by the caller).
+__global__ void __launch_bounds__(256) alphabetHistogram(const uint8_t* __restrict__ text, uint32_t total,
+                                                         TextSet texts, uint32_t* __restrict__ counts) {
+    __shared__ uint32_t h[256];
+    h[threadIdx.x] = 0;
+    __syncthreads();
+    const uint32_t lt = (1u << (threadIdx.x & 31)) - 1;
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x * 4;
+    for (uint64_t base = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) * 4; base < total;
+         base += stride) {
+        const uint32_t word = *reinterpret_cast<const uint32_t*>(text + base);
+        const uint32_t end = texts.endOf(static_cast<uint32_t>(base));
+#pragma unroll
+        for (int b = 0; b < 4; b++) {
+            const uint32_t c = base + b < end ? (word >> (8 * b)) & 0xFF : 0x100;
+            const uint32_t peers = __match_any_sync(0xffffffffu, c);
+            if (c != 0x100 && (peers & lt) == 0) atomicAdd(&h[c], static_cast<uint32_t>(__popc(peers)));
+        }
+    }
+    __syncthreads();
+    if (h[threadIdx.x]) atomicAdd(counts + threadIdx.x, h[threadIdx.x]);
+}
+
+// packed[w] = the 64 bits [64w, 64w + 64) of the code stream. One thread per word; positions past
+// the end of the concatenation read code 0.
+__global__ void packCodes(const uint8_t* __restrict__ text, uint32_t total, CodeTable table, uint32_t bits,
+                          uint64_t words, uint64_t* __restrict__ packed) {
+    const uint64_t w = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (w >= words) return;
+    const uint64_t firstBit = w * 64;
+    const uint64_t first = firstBit / bits, last = (firstBit + 63) / bits;
+    uint64_t out = 0;
+    for (uint64_t q = first; q <= last; q++) {
+        const uint64_t c = q < total ? table.code[text[q]] : 0;
+        // character q spans stream bits [q*bits, q*bits + bits); place it relative to this word
+        const int64_t shift = static_cast<int64_t>(firstBit + 64) - static_cast<int64_t>(q * bits + bits);
+        out |= shift >= 0 ? (shift < 64 ? c << shift : 0) : c >> (-shift);
+    }
+    packed[w] = out;
+}
+
+// 64 bits of the code stream starting at stream bit `bit`.
+__device__ __forceinline__ uint64_t streamBits(const uint64_t* __restrict__ packed, uint64_t bit) {
+    const uint64_t w = bit >> 6;
+    const uint32_t o = static_cast<uint32_t>(bit & 63);
+    const uint64_t hi = __ldg(packed + w);
+    return o ? (hi << o) | (__ldg(packed + w + 1) >> (64 - o)) : hi;
+}
+
+// Bits per character and characters per ranking key for an alphabet of sigma symbols.
+struct KeyShape {
+    uint32_t bits;      // per character
+    uint32_t chars;     // characters per 64-bit ranking key
+    uint32_t tagBits;   // length tag below them
+    uint32_t record;    // characters in a merge record's 128 bits
+};
+
+inline KeyShape keyShape(uint32_t sigma) {
+    KeyShape k{};
+    uint32_t b = 1;
+    while (b < 8 && (1u << b) < sigma) b++;
+    k.bits = b;
+    uint32_t c = 64 / b;
+    auto width = [](uint32_t x) {
+        uint32_t w = 0;
+        while (x) {
+            w++;
+            x >>= 1;
+        }
+        return w;
+    };
+    while (c * b + width(c) > 64) c--;
+    k.chars = c;
+    k.tagBits = width(c);
+    k.record = 128 / b;
+    return k;
+}
+
+// Number of stream words for a concatenation of `span` bytes, with room for 64-bit reads at any
+// position up to span + 64.
+inline uint64_t packedWords(uint64_t span, uint32_t bits) {
+    return ((span + 160) * bits + 63) / 64 + 4;
+}
+
+}  // namespace sadcs

@@ -141,6 +141,11 @@ struct TextSet {
     const uint32_t* end;
     uint32_t count;
     uint32_t oneEnd;
+    // The packed code stream (alphabet.cuh) and its shape.
+    const uint64_t* packed;
+    uint32_t bits;       // per character
+    uint32_t keyChars;   // characters per ranking key
+    uint32_t tagBits;    // length tag bits of a ranking key
     __device__ __forceinline__ uint32_t textOf(uint32_t p) const { return blockText ? __ldg(blockText + (p >> 5)) : 0; }
     __device__ __forceinline__ uint32_t endOf(uint32_t p) const {
         return blockText ? __ldg(end + __ldg(blockText + (p >> 5))) : oneEnd;

@@ -24,6 +24,7 @@
 // (all a comparison can need), and p. Comparisons reaching past 16 characters read the text.
 #pragma once
 
+#include "alphabet.cuh"
 #include "common.cuh"
 
 namespace sadcs {
@@ -41,8 +42,8 @@ struct __align__(16) MergeRow {
     uint32_t c[kClasses];
 };
 
-// w0, w1: the 16 text bytes at pos, big-endian; w2 is staging for the third aligned word while the
-// record is gathered (see gatherRecord). end: the end of pos's text (texts are ordered by it);
+// w0, w1: 128 bits of the code stream from pos (128 / bits characters); w2 is staging for the
+// third stream word while the record is gathered (see gatherRecord). end: the end of pos's text (texts are ordered by it);
 // text: its index.
 struct __align__(8) MergeRecord {
     uint64_t w0, w1, w2;
@@ -72,13 +73,16 @@ struct MergeArgs {
     uint32_t* error;         // set nonzero if a window set exceeds the capacity (never, by construction)
 };
 
-__device__ __forceinline__ uint64_t prefixMask(uint32_t c) {
-    return c >= 8 ? ~uint64_t(0) : (c == 0 ? uint64_t(0) : ~uint64_t(0) << (64 - 8 * c));
+// The top `bits` bits set (bits <= 64).
+__device__ __forceinline__ uint64_t topMask(uint32_t bits) {
+    return bits >= 64 ? ~uint64_t(0) : (bits == 0 ? uint64_t(0) : ~uint64_t(0) << (64 - bits));
 }
 
 __device__ __forceinline__ void loadRecord(const uint8_t* __restrict__ text, const uint32_t* __restrict__ ranks,
                                            const TextSet& texts, uint32_t p, MergeRecord& r) {
-    load16(text, p, r.w0, r.w1);
+    const uint64_t bit = static_cast<uint64_t>(p) * texts.bits;
+    r.w0 = streamBits(texts.packed, bit);
+    r.w1 = streamBits(texts.packed, bit + 64);
     const uint32_t base = pack(p);
 #pragma unroll
     for (int s = 0; s < kK; s++) r.rank[s] = __ldg(ranks + base + s);
@@ -94,34 +98,35 @@ struct MergeTables {
     uint8_t slot[kV][kV];
 };
 
-__device__ __forceinline__ bool lessRecord(const MergeRecord& a, const MergeRecord& b,
-                                           const uint8_t* __restrict__ text, const MergeTables& tb) {
+__device__ __forceinline__ bool lessRecord(const MergeRecord& a, const MergeRecord& b, const TextSet& texts,
+                                           const MergeTables& tb) {
     if (a.end != b.end) return a.end < b.end;  // different texts: text order
     const uint32_t n = a.end;
     const uint32_t i = a.pos, j = b.pos;
     const uint32_t k = tb.tie[i % kV][j % kV];
     const uint32_t common = min(k, min(n - i, n - j));
+    const uint32_t bits = common * texts.bits;
     uint64_t x = a.w0, y = b.w0;
-    if (common < 8) {
-        const uint64_t mk = prefixMask(common);
+    if (bits < 64) {
+        const uint64_t mk = topMask(bits);
         x &= mk;
         y &= mk;
     }
     if (x != y) return x < y;
-    if (common > 8) {
+    if (bits > 64) {
         x = a.w1;
         y = b.w1;
-        if (common < 16) {
-            const uint64_t mk = prefixMask(common - 8);
+        if (bits < 128) {
+            const uint64_t mk = topMask(bits - 64);
             x &= mk;
             y &= mk;
         }
         if (x != y) return x < y;
-        for (uint32_t o = 16; o < common; o += 8) {
-            x = load8(text, i + o);
-            y = load8(text, j + o);
-            if (common - o < 8) {
-                const uint64_t mk = prefixMask(common - o);
+        for (uint32_t o = 128; o < bits; o += 64) {
+            x = streamBits(texts.packed, static_cast<uint64_t>(i) * texts.bits + o);
+            y = streamBits(texts.packed, static_cast<uint64_t>(j) * texts.bits + o);
+            if (bits - o < 64) {
+                const uint64_t mk = topMask(bits - o);
                 x &= mk;
                 y &= mk;
             }
@@ -149,9 +154,9 @@ __device__ __forceinline__ void cpAsyncWaitAll() {
 // Issues the gather of r's raw text words (the three aligned words covering [p, p + 16)) and its
 // 7 sample ranks as asynchronous copies into shared memory: every load of every record of the
 // thread is in flight at once. finishRecord() turns the raw words into big-endian windows.
-__device__ __forceinline__ void gatherRecord(const uint8_t* __restrict__ text, const uint32_t* __restrict__ ranks,
-                                             const TextSet& texts, uint32_t p, MergeRecord& r) {
-    const uint64_t* words = reinterpret_cast<const uint64_t*>(text) + (p >> 3);
+__device__ __forceinline__ void gatherRecord(const uint32_t* __restrict__ ranks, const TextSet& texts, uint32_t p,
+                                             MergeRecord& r) {
+    const uint64_t* words = texts.packed + ((static_cast<uint64_t>(p) * texts.bits) >> 6);
     cpAsync8(&r.w0, words);
     cpAsync8(&r.w1, words + 1);
     cpAsync8(&r.w2, words + 2);
@@ -163,11 +168,11 @@ __device__ __forceinline__ void gatherRecord(const uint8_t* __restrict__ text, c
     r.end = texts.endOfText(r.text);
 }
 
-__device__ __forceinline__ void finishRecord(MergeRecord& r) {
-    const uint32_t shift = (r.pos & 7) * 8;
+__device__ __forceinline__ void finishRecord(MergeRecord& r, uint32_t bits) {
+    const uint32_t o = static_cast<uint32_t>((static_cast<uint64_t>(r.pos) * bits) & 63);
     const uint64_t a = r.w0, b = r.w1, c = r.w2;
-    r.w0 = byteSwap64(shift ? (a >> shift) | (b << (64 - shift)) : a);
-    r.w1 = byteSwap64(shift ? (b >> shift) | (c << (64 - shift)) : b);
+    r.w0 = o ? (a << o) | (b >> (64 - o)) : a;
+    r.w1 = o ? (b << o) | (c >> (64 - o)) : b;
 }
 
 struct MergeTileInfo {
@@ -295,7 +300,7 @@ __global__ void __launch_bounds__(kMergeThreads) mergeTiles(MergeArgs a) {
 #pragma unroll
     for (int j = 0; j < kItems; j++) {
         const uint32_t e = threadIdx.x + j * kMergeThreads;
-        if (e < size) gatherRecord(a.text, a.ranks, a.texts, pos[j], rec[e]);
+        if (e < size) gatherRecord(a.ranks, a.texts, pos[j], rec[e]);
     }
     uint32_t* cnt32 = reinterpret_cast<uint32_t*>(cnt);
     for (uint32_t i = threadIdx.x; i < size * 4; i += kMergeThreads) cnt32[i] = 0;
@@ -303,7 +308,7 @@ __global__ void __launch_bounds__(kMergeThreads) mergeTiles(MergeArgs a) {
 #pragma unroll
     for (int j = 0; j < kItems; j++) {
         const uint32_t e = threadIdx.x + j * kMergeThreads;
-        if (e < size) finishRecord(rec[e]);
+        if (e < size) finishRecord(rec[e], a.texts.bits);
     }
     __syncthreads();
 
@@ -319,7 +324,7 @@ __global__ void __launch_bounds__(kMergeThreads) mergeTiles(MergeArgs a) {
         uint32_t lo = d > lenB ? d - lenB : 0, hi = min(d, lenA);
         while (lo < hi) {
             const uint32_t mid = (lo + hi) >> 1;
-            if (lessRecord(rec[sa + mid], rec[sb + d - 1 - mid], a.text, tb)) {
+            if (lessRecord(rec[sa + mid], rec[sb + d - 1 - mid], a.texts, tb)) {
                 lo = mid + 1;
             } else {
                 hi = mid;
@@ -327,7 +332,7 @@ __global__ void __launch_bounds__(kMergeThreads) mergeTiles(MergeArgs a) {
         }
         uint32_t i = lo, j = d - lo;
         for (; d < end; d++) {
-            if (j == lenB || (i < lenA && lessRecord(rec[sa + i], rec[sb + j], a.text, tb))) {
+            if (j == lenB || (i < lenA && lessRecord(rec[sa + i], rec[sb + j], a.texts, tb))) {
                 cnt[(sa + i) * 8 + lb] = static_cast<uint16_t>(j);
                 i++;
             } else {
@@ -426,7 +431,7 @@ __global__ void mergeSuffixZeroRows(MergeArgs a, const uint32_t* __restrict__ ro
         const uint32_t mid = (lo + hi) >> 1;
         MergeRecord r;
         loadRecord(a.text, a.ranks, a.texts, list[mid], r);
-        if (lessRecord(r, zero, a.text, tb)) {
+        if (lessRecord(r, zero, a.texts, tb)) {
             lo = mid + 1;
         } else {
             hi = mid;

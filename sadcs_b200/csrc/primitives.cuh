@@ -435,6 +435,14 @@ struct RadixScratch {
         status = control + 64;
         (void)count;
     }
+    // Control words and status words at given places (no digit-base table).
+    static RadixScratch at(uint32_t* control, uint32_t* status) {
+        RadixScratch r(control, 0);
+        r.digitBase = nullptr;
+        r.control = control;
+        r.status = status;
+        return r;
+    }
 };
 
 // One pass over `tiles` tiles (ceilDiv(count, kSortTile) for one segment; the segment table's total

@@ -17,8 +17,13 @@
 // Every subkey of a pass is read before any id of that pass is written.
 #pragma once
 
+#include <cstdio>
+#include <cstdlib>
+
+#include "alphabet.cuh"
 #include "common.cuh"
 #include "primitives.cuh"
+#include "segsort.cuh"
 
 namespace sadcs {
 
@@ -30,17 +35,32 @@ struct RankBuffers {
     uint32_t* aux2;
     uint32_t* scratch;      // radix scratch words (radixScratchWords(m))
     uint32_t* scanScratch;  // scan scratch words (scanScratchWords(m))
-    uint32_t* counter;      // one device word
+    uint32_t* segScratch;   // segmented-sort scratch (segScratchWords(m))
+    uint32_t* counter;      // device words: [0] list count, [4..7] segmented sort
 };
 
-constexpr uint32_t kCharsPerPass = 7;
 
-__device__ __forceinline__ uint64_t charKey(const uint8_t* __restrict__ text, uint32_t n, uint32_t q) {
-    if (q >= n) return 0;
-    const uint32_t remaining = n - q;
-    const uint64_t chars = load8(text, q) & ~uint64_t(0xFF);
-    if (remaining >= kCharsPerPass) return chars | kCharsPerPass;
-    return (chars & (~uint64_t(0) << (64 - 8 * remaining))) | remaining;
+// SADCS_TRACE=1 in the environment: one line per ranking pass on stderr.
+inline bool traceEnabled() {
+    static const bool enabled = [] {
+        const char* v = std::getenv("SADCS_TRACE");
+        return v && v[0] && v[0] != '0';
+    }();
+    return enabled;
+}
+
+// The keyChars characters at q in the top bits and min(remaining, keyChars) in the low tagBits
+// bits; characters past the end read as code 0. Key width keyChars * bits + tagBits <= 64.
+__device__ __forceinline__ uint64_t charKey(const TextSet& texts, uint32_t end, uint32_t q) {
+    const uint32_t c = texts.keyChars, b = texts.bits;
+    const uint32_t remaining = end - q;
+    uint64_t v = streamBits(texts.packed, static_cast<uint64_t>(q) * b) >> (64 - c * b);
+    uint32_t tag = c;
+    if (remaining < c) {
+        v &= ~((uint64_t(1) << ((c - remaining) * b)) - 1);
+        tag = remaining;
+    }
+    return (v << texts.tagBits) | tag;
 }
 
 __global__ void rankInitList(uint32_t* __restrict__ lst, uint32_t m) {
@@ -61,7 +81,7 @@ __global__ void rankMakeKeys(const uint8_t* __restrict__ text, const uint32_t* _
     if (doubling) {
         key[i] = q < end ? static_cast<uint64_t>(ranks[pack(static_cast<uint32_t>(q))]) + 1 : 0;
     } else {
-        key[i] = q < end ? charKey(text, end, static_cast<uint32_t>(q)) : 0;
+        key[i] = q < end ? charKey(texts, end, static_cast<uint32_t>(q)) : 0;
     }
 }
 
@@ -172,6 +192,7 @@ inline cudaError_t rankSample(const uint8_t* text, const TextSet& texts, uint32_
     uint64_t depth = 0;
     bool first = texts.count <= 1;  // one text: everything starts in one group, no group sort
     const int rankBits = bitWidth(static_cast<uint64_t>(live) + 1);
+    const int charBits = static_cast<int>(texts.keyChars * texts.bits + texts.tagBits);
     while (u > 0) {
         const bool doubling = depth >= kV;
         const uint32_t offset = doubling ? static_cast<uint32_t>((depth / kV) * kV) : static_cast<uint32_t>(depth);
@@ -183,16 +204,18 @@ inline cudaError_t rankSample(const uint8_t* text, const TextSet& texts, uint32_
         uint64_t* keyAlt = b.key[1];
         SADCS_TRY(launch(rankMakeKeys, blocks256(u), 256, 0, stream, text, ranks, texts, lst, key, u, offset,
                          doubling ? 1 : 0));
-        SADCS_TRY(radixSortPairs<uint64_t>(key, keyAlt, lst, lstAlt, u, 0, doubling ? rankBits : 64, b.scratch, stream));
-        if (!first) {
-            // Stably by the old group id (the list keeps whole groups in id order), then recompute
-            // the subkeys in the new order; the subkey buffer is free for the group keys meanwhile.
-            SADCS_TRY(launch(rankGatherGroupKeys, blocks256(u), 256, 0, stream, ranks, lst, key, u, slots));
-            SADCS_TRY(radixSortPairs<uint64_t>(key, keyAlt, lst, lstAlt, u, 0, rankBits, b.scratch, stream));
-            SADCS_TRY(launch(rankMakeKeys, blocks256(u), 256, 0, stream, text, ranks, texts, lst, key, u, offset,
-                             doubling ? 1 : 0));
+        const int keyBits = doubling ? rankBits : charBits;
+        if (first) {
+            // Everything in one group: one global sort by subkey.
+            SADCS_TRY(radixSortPairs<uint64_t>(key, keyAlt, lst, lstAlt, u, 0, keyBits, b.scratch, stream));
+            SADCS_TRY(launch(rankGatherGroups, blocks256(u), 256, 0, stream, ranks, lst, b.grp, u, slots));
+        } else {
+            // The list holds whole groups in id order: sort inside each group only.
+            SADCS_TRY(launch(rankGatherGroups, blocks256(u), 256, 0, stream, ranks, lst, b.grp, u, slots));
+            SegBuffers sb{error - 1, b.aux1, b.aux2, reinterpret_cast<uint32_t*>(keyAlt), b.segScratch,
+                          b.counter + 4, b.scanScratch};
+            SADCS_TRY(segmentedSort(b.grp, u, key, lst, keyAlt, lstAlt, keyBits, sb, hostCounter + 8, stream));
         }
-        SADCS_TRY(launch(rankGatherGroups, blocks256(u), 256, 0, stream, ranks, lst, b.grp, u, slots));
         SADCS_TRY(launch(rankOldHeads, blocks256(u), 256, 0, stream, b.grp, b.aux1, u));
         SADCS_TRY((deviceScan<OpMax, true>(b.aux1, b.aux1, u, b.scanScratch, nullptr, stream)));
         SADCS_TRY(launch(rankNewHeads, blocks256(u), 256, 0, stream, b.grp, key, b.aux1, b.aux2, u));
@@ -204,6 +227,10 @@ inline cudaError_t rankSample(const uint8_t* text, const TextSet& texts, uint32_
         SADCS_TRY(cudaMemcpyAsync(hostCounter + 1, error, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
         SADCS_TRY(cudaStreamSynchronize(stream));
         if (hostCounter[1]) return cudaErrorLaunchTimeout;  // a radix look-back gave up
+        if (traceEnabled()) {
+            fprintf(stderr, "sadcs: ranking %s depth %llu: %u -> %u unresolved\n", doubling ? "doubling" : "characters",
+                    static_cast<unsigned long long>(depth), u, *hostCounter);
+        }
         u = *hostCounter;
         cur = lstAlt;
         alt = lst;
@@ -212,7 +239,7 @@ inline cudaError_t rankSample(const uint8_t* text, const TextSet& texts, uint32_
             depth += offset;
         } else {
             stats.characterPasses++;
-            depth += kCharsPerPass;
+            depth += texts.keyChars;
         }
         first = false;
     }

@@ -18,6 +18,7 @@
 #include <string>
 #include <vector>
 
+#include "alphabet.cuh"
 #include "bwt.cuh"
 #include "check.cuh"
 #include "classes.cuh"
@@ -112,9 +113,10 @@ size_t metaWords(uint32_t count, uint64_t span) {
 
 // Byte offsets of every buffer of a construction, and the peaks.
 struct Layout {
-    size_t text = 0, ranks = 0, meta = 0;
+    size_t text = 0, packed = 0, alphabet = 0, ranks = 0, meta = 0;
     // ranking region (the packed upload of a batch is staged at its start)
     size_t lst0 = 0, lst1 = 0, key0 = 0, key1 = 0, grp = 0, aux1 = 0, aux2 = 0, rankScratch = 0, scanScratch = 0;
+    size_t segScratch = 0;
     size_t counter = 0;
     // class + merge region (overlaps the ranking region)
     size_t lists = 0, classScratch = 0, splitters = 0, rows = 0, sa = 0, bwt = 0, mergeCounter = 0;
@@ -161,6 +163,8 @@ Layout planLayout(const Extent& x, bool internalSa, bool internalBwt) {
         return offset;
     };
     L.text = take(x.span + kTextPad);
+    L.packed = take(8 * packedWords(x.span, 8));
+    L.alphabet = take(4 * 256);
     L.ranks = take(4 * (x.slots + kRankPad));
     L.meta = take(4 * metaWords(x.count, x.span));
     const size_t persistent = at;
@@ -172,8 +176,9 @@ Layout planLayout(const Extent& x, bool internalSa, bool internalBwt) {
     L.key1 = take(8 * m);
     L.grp = take(4 * m);
     L.aux1 = take(4 * m);
-    L.aux2 = take(4 * m);
+    L.aux2 = take(4 * (m + 64));
     L.rankScratch = take(4 * radixScratchWords(m));
+    L.segScratch = take(4 * segScratchWords(m));
     L.scanScratch = take(4 * scanScratchWords(m));
     L.counter = take(256);
     L.rankingEnd = std::max(at, persistent + align256(x.outputs));
@@ -308,7 +313,7 @@ int createContext(int64_t capacity, uint32_t texts, sadcs_gpu_context** out) {
     c->maxTexts = texts;
     c->slabBytes = bytes;
     // counters, then the host copy of the tables (without the block map, built on the device)
-    c->hostWordCount = 64 + metaWords(texts, 0) + 2 * static_cast<size_t>(texts) + 64;
+    c->hostWordCount = 64 + metaWords(texts, 0) + 2 * static_cast<size_t>(texts) + 64 + 256;
     cudaError_t error;
     if ((error = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess ||
         (error = cudaMallocHost(&c->hostWords, 4 * c->hostWordCount)) != cudaSuccess ||
@@ -341,6 +346,33 @@ float elapsedMs(cudaEvent_t a, cudaEvent_t b) {
     float ms = 0;
     cudaEventElapsedTime(&ms, a, b);
     return ms;
+}
+
+// The alphabet of the placed texts, its key shape and the packed code stream (alphabet.cuh).
+// counts: 256 device words; hostCounts: 256 page-locked words. Fills texts' stream fields.
+cudaError_t prepareAlphabet(const uint8_t* text, uint64_t total, uint64_t span, uint32_t* counts, uint32_t* hostCounts,
+                            uint64_t* packed, TextSet& texts, cudaStream_t stream) {
+    SADCS_TRY(cudaMemsetAsync(counts, 0, 256 * 4, stream));
+    const uint32_t blocks = std::min<uint32_t>(ceilDiv(total + 3ull, 256 * 4 * 8), 148 * 8);
+    SADCS_TRY(launch(alphabetHistogram, std::max(blocks, 1u), 256, 0, stream, text, static_cast<uint32_t>(total), texts,
+                     counts));
+    SADCS_TRY(cudaMemcpyAsync(hostCounts, counts, 256 * 4, cudaMemcpyDeviceToHost, stream));
+    SADCS_TRY(cudaStreamSynchronize(stream));
+    CodeTable table{};
+    uint32_t sigma = 0;
+    for (int c = 0; c < 256; c++) {
+        table.code[c] = static_cast<uint8_t>(sigma);
+        if (hostCounts[c]) sigma++;
+    }
+    const KeyShape shape = keyShape(std::max(sigma, 1u));
+    const uint64_t words = packedWords(span, shape.bits);
+    SADCS_TRY(launch(packCodes, ceilDiv(words, 256), 256, 0, stream, text, static_cast<uint32_t>(total), table,
+                     shape.bits, words, packed));
+    texts.packed = packed;
+    texts.bits = shape.bits;
+    texts.keyChars = shape.chars;
+    texts.tagBits = shape.tagBits;
+    return cudaSuccess;
 }
 
 // Where a construction's inputs come from and its outputs go.
@@ -442,6 +474,14 @@ int construct(sadcs_gpu_context* c, const Batch& b, Io& io, cudaStream_t stream,
     start = std::chrono::steady_clock::now();
     cudaEventRecord(c->events[0], stream);
 
+    // The alphabet and the packed code stream.
+    const uint64_t scanned = J == 1 ? b.end[0] : b.end[J - 1];
+    if ((error = prepareAlphabet(text, scanned, b.span, reinterpret_cast<uint32_t*>(slab + L.alphabet),
+                                 c->hostWords + c->hostWordCount - 256, reinterpret_cast<uint64_t*>(slab + L.packed),
+                                 texts, stream)) != cudaSuccess) {
+        return failed("alphabet", error);
+    }
+
     // Sample ranking.
     if (J == 1 && (error = cudaMemsetAsync(ranks, 0, 4 * (b.slots + kRankPad), stream)) != cudaSuccess) {
         return failed("ranking", error);
@@ -459,6 +499,7 @@ int construct(sadcs_gpu_context* c, const Batch& b, Io& io, cudaStream_t stream,
     rb.aux2 = reinterpret_cast<uint32_t*>(slab + L.aux2);
     rb.scratch = reinterpret_cast<uint32_t*>(slab + L.rankScratch);
     rb.scanScratch = reinterpret_cast<uint32_t*>(slab + L.scanScratch);
+    rb.segScratch = reinterpret_cast<uint32_t*>(slab + L.segScratch);
     rb.counter = reinterpret_cast<uint32_t*>(slab + L.counter);
     RankStats rankStats;
     if ((error = rankSample(text, texts, static_cast<uint32_t>(b.slots), static_cast<uint32_t>(b.live), dSampleBase,
@@ -936,10 +977,17 @@ int sadcs_gpu_rank_sample(const uint8_t* text, int64_t n, uint32_t* ranks, sadcs
         rb.aux2 = reinterpret_cast<uint32_t*>(c->slab + L.aux2);
         rb.scratch = reinterpret_cast<uint32_t*>(c->slab + L.rankScratch);
         rb.scanScratch = reinterpret_cast<uint32_t*>(c->slab + L.scanScratch);
+        rb.segScratch = reinterpret_cast<uint32_t*>(c->slab + L.segScratch);
         rb.counter = reinterpret_cast<uint32_t*>(c->slab + L.counter);
         TextSet texts{};
         texts.count = 1;
         texts.oneEnd = static_cast<uint32_t>(length);
+        if ((error = prepareAlphabet(textBuffer, length, b.span, reinterpret_cast<uint32_t*>(c->slab + L.alphabet),
+                                     c->hostWords + c->hostWordCount - 256,
+                                     reinterpret_cast<uint64_t*>(c->slab + L.packed), texts, c->stream)) !=
+            cudaSuccess) {
+            return failed("alphabet", error);
+        }
         RankStats rankStats;
         if ((error = rankSample(textBuffer, texts, static_cast<uint32_t>(b.slots), static_cast<uint32_t>(b.live),
                                 nullptr, static_cast<uint32_t>(length), rankBuffer, rb, c->hostWords, c->stream,

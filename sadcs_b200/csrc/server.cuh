@@ -140,7 +140,7 @@ void serverWorker(sadcs_gpu_server* srv) {
     cudaSetDevice(srv->device);
     sadcs_gpu_context ctx;
     ctx.device = srv->device;
-    ctx.hostWordCount = 64 + metaWords(srv->batchTexts, 0) + 2 * static_cast<size_t>(srv->batchTexts) + 64;
+    ctx.hostWordCount = 64 + metaWords(srv->batchTexts, 0) + 2 * static_cast<size_t>(srv->batchTexts) + 64 + 256;
     uint8_t* staging = nullptr;
     bool ready = cudaStreamCreateWithFlags(&ctx.stream, cudaStreamNonBlocking) == cudaSuccess &&
                  cudaMallocHost(&ctx.hostWords, 4 * ctx.hostWordCount) == cudaSuccess &&
