@@ -186,6 +186,17 @@ int sadcs_gpu_server_wait(sadcs_gpu_server* server, uint64_t ticket, double time
 void sadcs_gpu_server_counters(sadcs_gpu_server* server, int64_t* constructions, int64_t* launches);
 void sadcs_gpu_server_destroy(sadcs_gpu_server* server);
 
+/* No counterpart: the reference's BWT check (src/common/checker.cpp:196-245) on the device: inverts
+ * d_bwt (n bytes, primary) and compares with d_text. *bad_index = -1 if correct, else the first text
+ * position that differs (0 if the BWT does not invert at all). Uses about 25n bytes of temporary
+ * device memory. */
+int sadcs_gpu_check_bwt(const uint8_t* d_text, int64_t n, const uint8_t* d_bwt, int64_t primary, int64_t* bad_index,
+                        void* stream);
+
+/* No counterpart: the inverse BWT (unbwt) on the device: d_text (n bytes) from d_bwt and primary.
+ * Returns SADCS_FAILED if d_bwt is not a valid BWT. */
+int sadcs_gpu_inverse_bwt(const uint8_t* d_bwt, int64_t n, int64_t primary, uint8_t* d_text, void* stream);
+
 /* No counterpart: the capacity (bytes of text) of a context. */
 int64_t sadcs_gpu_context_capacity(const sadcs_gpu_context* context);
 

@@ -148,6 +148,12 @@ def lib() -> ctypes.CDLL:
         L.sadcs_gpu_server_counters.argtypes = [ctypes.c_void_p, _i64p, _i64p]
         L.sadcs_gpu_server_destroy.restype = None
         L.sadcs_gpu_server_destroy.argtypes = [ctypes.c_void_p]
+        L.sadcs_gpu_check_bwt.restype = ctypes.c_int
+        L.sadcs_gpu_check_bwt.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64, _i64p,
+                                          ctypes.c_void_p]
+        L.sadcs_gpu_inverse_bwt.restype = ctypes.c_int
+        L.sadcs_gpu_inverse_bwt.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_void_p,
+                                            ctypes.c_void_p]
         L.sadcs_gpu_check_suffix_array.restype = ctypes.c_int
         L.sadcs_gpu_check_suffix_array.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, _i64p,
                                                    ctypes.POINTER(ctypes.c_char_p), ctypes.c_void_p]
@@ -359,6 +365,20 @@ def check_suffix_array_device(d_text: int, n: int, d_sa: int, stream: int | None
                                               ctypes.byref(index), ctypes.byref(reason),
                                               ctypes.c_void_p(stream) if stream else None))
     return index.value < 0, int(index.value), reason.value.decode() if reason.value else None
+
+
+def check_bwt_device(d_text: int, n: int, d_bwt: int, primary: int, stream: int | None = None):
+    """The reference's BWT check on device buffers: (ok, first failing text position)."""
+    index = ctypes.c_int64(-1)
+    _check(lib().sadcs_gpu_check_bwt(ctypes.c_void_p(d_text), int(n), ctypes.c_void_p(d_bwt), int(primary),
+                                     ctypes.byref(index), ctypes.c_void_p(stream) if stream else None))
+    return index.value < 0, int(index.value)
+
+
+def inverse_bwt_device(d_bwt: int, n: int, primary: int, d_text: int, stream: int | None = None) -> None:
+    """unbwt on device buffers: d_text (n bytes) from the BWT and its primary index."""
+    _check(lib().sadcs_gpu_inverse_bwt(ctypes.c_void_p(d_bwt), int(n), int(primary), ctypes.c_void_p(d_text),
+                                       ctypes.c_void_p(stream) if stream else None))
 
 
 def allocate_pinned(nbytes: int) -> np.ndarray:

@@ -940,6 +940,92 @@ int sadcs_gpu_check_suffix_array(const uint8_t* d_text, int64_t n, const uint32_
     return SADCS_OK;
 }
 
+namespace {
+
+// Inverse BWT into d_out with temporary device memory; valid = false for a broken BWT.
+int inverseWithScratch(const uint8_t* d_bwt, int64_t n, int64_t primary, uint8_t* d_out, cudaStream_t st, bool& valid) {
+    uint32_t* scratch = nullptr;
+    uint32_t* host = nullptr;
+    cudaError_t error;
+    if ((error = cudaMallocAsync(&scratch, 4 * inverseScratchWords(static_cast<uint64_t>(n)), st)) != cudaSuccess) {
+        return failed("cudaMallocAsync", error);
+    }
+    if ((error = cudaMallocHost(&host, 16)) != cudaSuccess) {
+        cudaFreeAsync(scratch, st);
+        return failed("cudaMallocHost", error);
+    }
+    error = inverseBwt(d_bwt, static_cast<uint32_t>(n), static_cast<uint32_t>(primary), d_out, scratch, host, st, valid);
+    cudaFreeAsync(scratch, st);
+    cudaStreamSynchronize(st);
+    cudaFreeHost(host);
+    return error == cudaSuccess ? SADCS_OK : failed("inverse BWT", error);
+}
+
+}  // namespace
+
+int sadcs_gpu_inverse_bwt(const uint8_t* d_bwt, int64_t n, int64_t primary, uint8_t* d_text, void* stream) {
+    tLastError[0] = '\0';
+    if (n <= 0) return SADCS_OK;
+    if (n > kMaxText || primary < 1 || primary > n) {
+        setError("invalid BWT: n %lld, primary %lld", static_cast<long long>(n), static_cast<long long>(primary));
+        return SADCS_FAILED;
+    }
+    bool valid = true;
+    const int status = inverseWithScratch(d_bwt, n, primary, d_text, static_cast<cudaStream_t>(stream), valid);
+    if (status == SADCS_OK && !valid) {
+        setError("not a valid BWT: LF misses the primary row");
+        return SADCS_FAILED;
+    }
+    return status;
+}
+
+int sadcs_gpu_check_bwt(const uint8_t* d_text, int64_t n, const uint8_t* d_bwt, int64_t primary, int64_t* bad_index,
+                        void* stream) {
+    tLastError[0] = '\0';
+    if (bad_index) *bad_index = -1;
+    if (n <= 0) {
+        if (bad_index && primary != 0) *bad_index = 0;
+        return SADCS_OK;
+    }
+    if (n > kMaxText) {
+        setError("text of %lld bytes exceeds the limit of %lld", static_cast<long long>(n), static_cast<long long>(kMaxText));
+        return SADCS_FAILED;
+    }
+    if (primary < 1 || primary > n) {
+        if (bad_index) *bad_index = 0;
+        return SADCS_OK;
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    uint8_t* inverse = nullptr;
+    unsigned long long* word = nullptr;
+    unsigned long long host = 0;
+    cudaError_t error;
+    if ((error = cudaMallocAsync(&inverse, static_cast<size_t>(n), st)) != cudaSuccess ||
+        (error = cudaMallocAsync(&word, 8, st)) != cudaSuccess) {
+        if (inverse) cudaFreeAsync(inverse, st);
+        return failed("cudaMallocAsync", error);
+    }
+    bool valid = true;
+    int status = inverseWithScratch(d_bwt, n, primary, inverse, st, valid);
+    if (status == SADCS_OK && valid) {
+        if ((error = cudaMemsetAsync(word, 0xFF, 8, st)) != cudaSuccess ||
+            (error = launch(lfCompare, ceilDiv(n, 256), 256, 0, st, d_text, inverse, static_cast<uint32_t>(n), word)) !=
+                cudaSuccess ||
+            (error = cudaMemcpyAsync(&host, word, 8, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+            (error = cudaStreamSynchronize(st)) != cudaSuccess) {
+            status = failed("BWT check", error);
+        } else if (bad_index && host != kNoFailure) {
+            *bad_index = static_cast<int64_t>(host);
+        }
+    } else if (status == SADCS_OK && bad_index) {
+        *bad_index = 0;
+    }
+    cudaFreeAsync(inverse, st);
+    cudaFreeAsync(word, st);
+    cudaStreamSynchronize(st);
+    return status;
+}
+
 int sadcs_gpu_rank_sample(const uint8_t* text, int64_t n, uint32_t* ranks, sadcs_gpu_stats* stats) {
     tLastError[0] = '\0';
     sadcs_gpu_stats local{};

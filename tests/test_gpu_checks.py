@@ -1,0 +1,62 @@
+"""Device-side checkers and the inverse BWT: they accept what the oracle accepts and catch the
+reference selftest's planted errors (src/cli/selftest.cpp:309-385)."""
+import numpy as np
+import pytest
+
+import oracle
+import sadcs_b200 as sa
+from sadcs_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def _device(a):
+    import torch
+
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def test_suffix_array_check_accepts_and_rejects():
+    rng = W.SplitMix(7)
+    text = W.random_text(rng, 3000, 3)
+    good = oracle.naive_sa(text)
+    d_text = _device(text)
+    ok, index, _ = sa.check_suffix_array_device(d_text.data_ptr(), len(text), _device(good).data_ptr())
+    assert ok and index == -1
+    mutations = {
+        "swapped neighbours": lambda s: s.__setitem__(slice(1000, 1002), s[1000:1002][::-1].copy()),
+        "swapped far apart": lambda s: s.__setitem__([10, 2900], s[[2900, 10]]),
+        "duplicate entry": lambda s: s.__setitem__(500, s[1500]),
+        "out of range": lambda s: s.__setitem__(42, len(s)),
+    }
+    for name, mutate in mutations.items():
+        bad = good.copy()
+        mutate(bad)
+        ok, index, reason = sa.check_suffix_array_device(d_text.data_ptr(), len(text), _device(bad).data_ptr())
+        assert not ok and index >= 0 and reason, name
+
+
+def test_bwt_check_and_inverse():
+    import torch
+
+    for text in (W.natural_text(1 << 20, seed=3), W.run_text(5000), W.fibonacci_text(9000),
+                 np.frombuffer(b"mississippi", np.uint8), W.random_text(W.SplitMix(2), 70000, 256)):
+        expected = oracle.doubling_sa(text)
+        bwt, primary = oracle.bwt_from_sa(text, expected)
+        d_text, d_bwt = _device(text), _device(bwt)
+        ok, index = sa.check_bwt_device(d_text.data_ptr(), len(text), d_bwt.data_ptr(), primary)
+        assert ok and index == -1
+        out = torch.zeros(len(text), dtype=torch.uint8, device="cuda")
+        sa.inverse_bwt_device(d_bwt.data_ptr(), len(text), primary, out.data_ptr())
+        torch.cuda.synchronize()
+        assert np.array_equal(out.cpu().numpy(), text)
+    text = W.random_text(W.SplitMix(7), 3000, 3)
+    bwt, primary = oracle.bwt_from_sa(text, oracle.naive_sa(text))
+    changed = bwt.copy()
+    changed[1234] ^= 1
+    d_text = _device(text)
+    for name, b, p in (("changed character", changed, primary),
+                       ("primary off by one", bwt, primary + 1 if primary < 3000 else primary - 1),
+                       ("primary 0", bwt, 0)):
+        ok, _ = sa.check_bwt_device(d_text.data_ptr(), len(text), _device(b).data_ptr(), p)
+        assert not ok, name
