@@ -26,12 +26,16 @@ __global__ void __launch_bounds__(256) alphabetHistogram(const uint8_t* __restri
     __shared__ uint32_t h[256];
     h[threadIdx.x] = 0;
     __syncthreads();
-    const uint32_t lt = (1u << (threadIdx.x & 31)) - 1;
+    const uint32_t lane = threadIdx.x & 31, lt = (1u << lane) - 1;
     const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x * 4;
-    for (uint64_t base = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) * 4; base < total;
-         base += stride) {
-        const uint32_t word = *reinterpret_cast<const uint32_t*>(text + base);
-        const uint32_t end = texts.endOf(static_cast<uint32_t>(base));
+    // The loop runs on the warp's base, so every lane of a warp makes the same number of trips (the
+    // match below names all 32 lanes).
+    for (uint64_t warpBase = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + (threadIdx.x - lane)) * 4;
+         warpBase < total; warpBase += stride) {
+        const uint64_t base = warpBase + lane * 4;
+        const bool any = base < total;
+        const uint32_t word = any ? *reinterpret_cast<const uint32_t*>(text + base) : 0;
+        const uint32_t end = any ? texts.endOf(static_cast<uint32_t>(base)) : 0;
 #pragma unroll
         for (int b = 0; b < 4; b++) {
             const uint32_t c = base + b < end ? (word >> (8 * b)) & 0xFF : 0x100;
@@ -67,6 +71,16 @@ __device__ __forceinline__ uint64_t streamBits(const uint64_t* __restrict__ pack
     const uint32_t o = static_cast<uint32_t>(bit & 63);
     const uint64_t hi = __ldg(packed + w);
     return o ? (hi << o) | (__ldg(packed + w + 1) >> (64 - o)) : hi;
+}
+
+// The code of character q.
+__device__ __forceinline__ uint32_t charCode(const TextSet& texts, uint64_t q) {
+    return static_cast<uint32_t>(streamBits(texts.packed, q * texts.bits) >> (64 - texts.bits));
+}
+
+// The byte of character q.
+__device__ __forceinline__ uint8_t charByte(const TextSet& texts, uint64_t q) {
+    return __ldg(texts.decode + charCode(texts, q));
 }
 
 // Bits per character and characters per ranking key for an alphabet of sigma symbols.

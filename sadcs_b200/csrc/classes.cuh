@@ -15,6 +15,7 @@
 
 #include <algorithm>
 
+#include "alphabet.cuh"
 #include "common.cuh"
 #include "primitives.cuh"
 
@@ -117,7 +118,7 @@ struct ClassLoader {
         const uint32_t p = k == 0 ? end : lists[__ldg(prevOffset + j) + k - 1];
         if (p <= start || p > end || cCover.classOf[(p - 1) % kV] != d) return false;
         v = p - 1;
-        dig = text[v];
+        dig = charCode(texts, v);  // codes order like the bytes they stand for
         key = static_cast<uint8_t>(dig);
         return true;
     }
@@ -131,25 +132,29 @@ struct ClassStorer {
     }
 };
 
-// hist[(d * J + j) * 256 + c] = positions q of text j in class d with T[q] = c (zeroed by the caller).
-__global__ void __launch_bounds__(256) classHistogram(const uint8_t* __restrict__ text, uint32_t total,
-                                                      TextSet texts, uint32_t* __restrict__ hist) {
+// hist[(d * J + j) * 256 + c] = positions q of text j in class d with code c (zeroed by the caller).
+// Eight characters per thread from one 64-bit read of the code stream.
+__global__ void __launch_bounds__(256) classHistogram(uint32_t total, TextSet texts, uint32_t* __restrict__ hist) {
     __shared__ uint32_t h[kClasses * 256];
     const bool one = texts.count <= 1;
     for (int i = threadIdx.x; i < kClasses * 256; i += blockDim.x) h[i] = 0;
     __syncthreads();
-    const uint32_t lt = (1u << (threadIdx.x & 31)) - 1;
-    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x * 4;
-    for (uint64_t base = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) * 4; base < total;
-         base += stride) {
-        // four consecutive characters per thread, one 32-bit load (the text buffer is padded)
-        const uint32_t word = *reinterpret_cast<const uint32_t*>(text + base);
-        const uint32_t j = texts.textOf(static_cast<uint32_t>(base));
-        const uint32_t end = texts.endOfText(j);
+    const uint32_t lane = threadIdx.x & 31, lt = (1u << lane) - 1;
+    const uint32_t b = texts.bits;
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x * 8;
+    // The loop runs on the warp's base, so every lane of a warp makes the same number of trips (the
+    // match below names all 32 lanes).
+    for (uint64_t warpBase = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + (threadIdx.x - lane)) * 8;
+         warpBase < total; warpBase += stride) {
+        const uint64_t base = warpBase + lane * 8;
+        const bool any = base < total;
+        const uint64_t chunk = any ? streamBits(texts.packed, base * b) : 0;
+        const uint32_t j = any ? texts.textOf(static_cast<uint32_t>(base)) : 0;
+        const uint32_t end = any ? texts.endOfText(j) : 0;
 #pragma unroll
-        for (int b = 0; b < 4; b++) {
-            const uint64_t q = base + b;
-            const uint32_t c = (word >> (8 * b)) & 0xFF;
+        for (int k = 0; k < 8; k++) {
+            const uint64_t q = base + k;
+            const uint32_t c = static_cast<uint32_t>(chunk >> (64 - (k + 1) * b)) & ((1u << b) - 1);
             const uint32_t cls = q < end ? cCover.classOf[q % kV] : 0;
             const uint32_t key = cls ? (cls * texts.count + j) * 256 + c : 0xFFFFFFFFu;
             const uint32_t peers = __match_any_sync(0xffffffffu, key);
@@ -195,8 +200,8 @@ inline cudaError_t sortClasses(const uint8_t* text, uint32_t total, const TextSe
     const RadixScratch radix(classRadixScratch(scratch, J), 0);
     SADCS_TRY(cudaMemsetAsync(hist, 0, static_cast<size_t>(kClasses) * J * 256 * 4, stream));
     SADCS_TRY(cudaMemsetAsync(radix.control, 0, 8, stream));
-    const uint32_t blocks = std::min<uint32_t>(ceilDiv(total + 3ull, 256 * 4 * 8), 148 * 8);
-    SADCS_TRY(launch(classHistogram, blocks, 256, 0, stream, text, total, texts, hist));
+    const uint32_t blocks = std::min<uint32_t>(ceilDiv(total + 7ull, 256 * 8 * 8), 148 * 8);
+    SADCS_TRY(launch(classHistogram, std::max(blocks, 1u), 256, 0, stream, total, texts, hist));
     SADCS_TRY(launch(classDigitBase, kClasses * J, 256, 0, stream, hist, tables.rowBase));
     for (int d = 1; d < kClasses; d++) {
         if (plan.start[d + 1] == plan.start[d]) continue;

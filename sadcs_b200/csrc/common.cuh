@@ -141,8 +141,9 @@ struct TextSet {
     const uint32_t* end;
     uint32_t count;
     uint32_t oneEnd;
-    // The packed code stream (alphabet.cuh) and its shape.
+    // The packed code stream (alphabet.cuh), its shape, and code -> byte.
     const uint64_t* packed;
+    const uint8_t* decode;
     uint32_t bits;       // per character
     uint32_t keyChars;   // characters per ranking key
     uint32_t tagBits;    // length tag bits of a ranking key

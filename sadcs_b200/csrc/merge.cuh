@@ -371,7 +371,7 @@ __global__ void __launch_bounds__(kMergeThreads) mergeTiles(MergeArgs a) {
             if (a.sa) a.sa[g] = p - first;
             if (a.bwt && p != first) {
                 const uint32_t base = __ldg(a.outBase + tj), row = g - base, zero = __ldg(a.rowZero + tj);
-                a.bwt[base + (row < zero ? row + 1 : row)] = a.text[p - 1];
+                a.bwt[base + (row < zero ? row + 1 : row)] = charByte(a.texts, p - 1);
             }
         } else {
             if (g % kMergeR == 0) {
@@ -444,7 +444,7 @@ __global__ void mergeSuffixZeroRows(MergeArgs a, const uint32_t* __restrict__ ro
 __global__ void mergeBwtHeads(const uint8_t* __restrict__ text, TextSet texts, const uint32_t* __restrict__ outBase,
                               uint8_t* bwt) {
     const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j < texts.count) bwt[outBase[j]] = text[texts.endOfText(j) - 1];
+    if (j < texts.count) bwt[outBase[j]] = charByte(texts, texts.endOfText(j) - 1);
 }
 
 // Sizes of every level, planned on the host from n alone.

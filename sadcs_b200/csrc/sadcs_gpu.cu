@@ -113,7 +113,8 @@ size_t metaWords(uint32_t count, uint64_t span) {
 
 // Byte offsets of every buffer of a construction, and the peaks.
 struct Layout {
-    size_t text = 0, packed = 0, alphabet = 0, ranks = 0, meta = 0;
+    size_t packed = 0, alphabet = 0, ranks = 0, meta = 0;
+    size_t text = 0, staging = 0;  // raw bytes: dead once packed, so they share the ranking region
     // ranking region (the packed upload of a batch is staged at its start)
     size_t lst0 = 0, lst1 = 0, key0 = 0, key1 = 0, grp = 0, aux1 = 0, aux2 = 0, rankScratch = 0, scanScratch = 0;
     size_t segScratch = 0;
@@ -162,12 +163,15 @@ Layout planLayout(const Extent& x, bool internalSa, bool internalBwt) {
         at += align256(bytes);
         return offset;
     };
-    L.text = take(x.span + kTextPad);
     L.packed = take(8 * packedWords(x.span, 8));
     L.alphabet = take(4 * 256);
     L.ranks = take(4 * (x.slots + kRankPad));
     L.meta = take(4 * metaWords(x.count, x.span));
     const size_t persistent = at;
+    L.text = take(x.span + kTextPad);
+    L.staging = x.count > 1 ? take(x.outputs) : 0;
+    const size_t rawEnd = at;
+    at = persistent;
 
     const uint64_t m = x.live;
     L.lst0 = take(4 * m);
@@ -181,7 +185,7 @@ Layout planLayout(const Extent& x, bool internalSa, bool internalBwt) {
     L.segScratch = take(4 * segScratchWords(m));
     L.scanScratch = take(4 * scanScratchWords(m));
     L.counter = take(256);
-    L.rankingEnd = std::max(at, persistent + align256(x.outputs));
+    L.rankingEnd = std::max(at, rawEnd);
 
     at = persistent;
     L.lists = take(4 * x.outputs);
@@ -358,17 +362,25 @@ cudaError_t prepareAlphabet(const uint8_t* text, uint64_t total, uint64_t span, 
                      counts));
     SADCS_TRY(cudaMemcpyAsync(hostCounts, counts, 256 * 4, cudaMemcpyDeviceToHost, stream));
     SADCS_TRY(cudaStreamSynchronize(stream));
+    // Code k stands for the k-th byte present (in byte order); codes past sigma decode to 0.
     CodeTable table{};
+    uint8_t decodeTable[256] = {};
     uint32_t sigma = 0;
     for (int c = 0; c < 256; c++) {
         table.code[c] = static_cast<uint8_t>(sigma);
-        if (hostCounts[c]) sigma++;
+        if (hostCounts[c]) decodeTable[sigma++] = static_cast<uint8_t>(c);
     }
+    uint8_t* decodeHost = reinterpret_cast<uint8_t*>(hostCounts);  // the counts are read by now
+    memcpy(decodeHost, decodeTable, sizeof decodeTable);
+    uint8_t* decode = reinterpret_cast<uint8_t*>(counts);
+    SADCS_TRY(cudaMemcpyAsync(decode, decodeHost, 256, cudaMemcpyHostToDevice, stream));
     const KeyShape shape = keyShape(std::max(sigma, 1u));
     const uint64_t words = packedWords(span, shape.bits);
     SADCS_TRY(launch(packCodes, ceilDiv(words, 256), 256, 0, stream, text, static_cast<uint32_t>(total), table,
                      shape.bits, words, packed));
+    SADCS_TRY(cudaStreamSynchronize(stream));  // the decode table's host words are reused by the caller
     texts.packed = packed;
+    texts.decode = decode;
     texts.bits = shape.bits;
     texts.keyChars = shape.chars;
     texts.tagBits = shape.tagBits;
@@ -450,8 +462,8 @@ int construct(sadcs_gpu_context* c, const Batch& b, Io& io, cudaStream_t stream,
             return failed("upload", error);
         }
     } else {
-        uint8_t* staging = slab + L.lst0;
-        uint32_t* packedOffset = reinterpret_cast<uint32_t*>(slab + L.classScratch);  // free until the classes
+        uint8_t* staging = slab + L.staging;
+        uint32_t* packedOffset = reinterpret_cast<uint32_t*>(slab + L.packed);  // free until the codes are packed
         if ((error = cudaMemcpyAsync(staging, source, b.outputs,
                                      io.hostText ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, stream)) !=
                 cudaSuccess ||

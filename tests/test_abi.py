@@ -56,7 +56,7 @@ def test_required_bytes_plan():
         previous = need
     # SA + BWT from one construction: text, packed codes, ranks, lists, SA, BWT and small arrays.
     per_byte = sa.required_bytes(256 << 20) / (256 << 20)
-    assert 10.0 < per_byte < 12.5
+    assert 10.0 < per_byte < 11.5
     assert sa.memory_reserve() == 256 << 20
 
 
