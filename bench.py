@@ -52,6 +52,9 @@ WORKLOADS = {
     "natural256m": ("256 MiB natural-language-like text: 50k-word lowercase vocabulary (lengths 2-12), "
                     "Zipf(1.1) words, '.\\n' every 10-30 words, 2% capitalised, seed 2",
                     lambda W: W.natural_text(256 << 20, seed=2)),
+    "natural64m": ("64 MiB natural-language-like text, as natural256m (the profiling case: its merge reads "
+                   "3.4 GB, far above L2, with 0.75 GB on the device)",
+                   lambda W: W.natural_text(64 << 20, seed=2)),
     "uniform8m": ("8 MiB i.i.d. uniform bytes, seed 1", lambda W: W.uniform_bytes(8 << 20, seed=1)),
     "genome3g": ("3 GiB {A,C,G,T}: 2 GiB i.i.d. GC 0.41, then 1 GiB of mutated copies of 1 MiB segments "
                  "(1% substitutions, 0.1% indels of 1-10), seed 3", lambda W: W.genome_text(3 << 30, seed=3)),
