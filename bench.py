@@ -133,15 +133,24 @@ class ClockSampler:
 
 # ---- distributed plumbing -----------------------------------------------------------------------
 
+def rank_env():
+    """(world, rank, local rank) from the launcher's environment (1, 0, 0 without one)."""
+    return (int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
 def dist_setup(gpus: int):
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    """Joins the process group of a multi-GPU run. Ranks are independent replicas (one text, batch
+    or request stream each, no data-path collective); the group only carries the barriers around
+    the timed region and the max/sum of the per-rank results. NCCL on GPUs; gloo where SADCS_DIST_BACKEND
+    says so (the CPU tests of this host logic)."""
+    world, rank, local = rank_env()
     if world > 1:
         import torch.distributed as dist
         from datetime import timedelta
 
-        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+        backend = os.environ.get("SADCS_DIST_BACKEND", "nccl")
+        dist.init_process_group(backend, timeout=timedelta(seconds=300))
     return world, rank, local
 
 
@@ -152,26 +161,29 @@ def barrier(world):
         dist.barrier()
 
 
-def max_over_ranks(value: float, world: int) -> float:
+def _all_reduce(value: float, world: int, op: str) -> float:
     if world == 1:
         return value
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    device = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
     return float(t.item())
+
+
+def max_over_ranks(value: float, world: int) -> float:
+    return _all_reduce(value, world, "max")
 
 
 def sum_over_ranks(value: float, world: int) -> float:
-    if world == 1:
-        return value
-    import torch
-    import torch.distributed as dist
+    return _all_reduce(value, world, "sum")
 
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
+
+def rank_seed(base: int, rank: int) -> int:
+    """Seed of a rank's own synthetic batch or request stream (weak scaling: each rank its own)."""
+    return base + 1000 * rank
 
 
 # ---- CPU baseline (the reference's own CPU variant, or the oracle port) ----------------------------
@@ -434,7 +446,7 @@ def run_batch(args, world, rank, local) -> None:
     from sadcs_b200 import workloads as W
 
     torch.cuda.set_device(local)
-    texts = W.batch_texts(args.batch_count, lo=1 << 10, hi=4 << 20, seed=4 + rank)
+    texts = W.batch_texts(args.batch_count, lo=1 << 10, hi=4 << 20, seed=rank_seed(4, rank))
     lengths = [len(t) for t in texts]
     total = sum(lengths)
     packed = torch.from_numpy(np.concatenate(texts)).to(f"cuda:{local}")
@@ -508,7 +520,7 @@ def run_serve(args, world, rank, local) -> None:
     import sadcs_b200 as sa
 
     torch.cuda.set_device(local)
-    rng = np.random.default_rng(5 + rank)
+    rng = np.random.default_rng(rank_seed(5, rank))
     loads = [float(x) for x in args.serve_loads.split(",")]
     results = []
     for load in loads:
@@ -608,16 +620,20 @@ def main() -> None:
     p.add_argument("--no-e2e", dest="e2e", action="store_false")
     p.add_argument("--no-verify", dest="verify", action="store_false")
     args = p.parse_args()
+    if args.impl == "reference":
+        # Rank 0 alone times the reference on the host cores; other ranks exit without work (and
+        # without joining a process group, so nothing waits on them).
+        world, rank, _ = rank_env()
+        if args.workload in ("batch4096", "serve"):
+            if rank == 0:
+                print(json.dumps({"impl": "reference", "unavailable": "the reference has no batched or served "
+                                  "construction (one text per call); its per-text CPU rate is the natural256m line"}))
+        else:
+            run_reference(args, world, rank)
+        return
     world, rank, local = dist_setup(args.gpus)
     try:
-        if args.impl == "reference":
-            if args.workload in ("batch4096", "serve"):
-                if rank == 0:
-                    print(json.dumps({"impl": "reference", "unavailable": "the reference has no batched or served "
-                                      "construction (one text per call); its per-text CPU rate is the natural256m line"}))
-            else:
-                run_reference(args, world, rank)
-        elif args.workload == "batch4096":
+        if args.workload == "batch4096":
             run_batch(args, world, rank, local)
         elif args.workload == "serve":
             run_serve(args, world, rank, local)

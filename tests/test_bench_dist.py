@@ -1,0 +1,80 @@
+"""The multi-rank host logic of bench.py on CPU: world size 2 over gloo.
+
+A single text does not shard, so N ranks build N independent replicas (or N independent batches and
+request streams); the process group only carries the barriers and the max/sum of per-rank results.
+These tests run that plumbing with two CPU processes, no GPU.
+"""
+import json
+import os
+import socket
+import subprocess
+import sys
+from pathlib import Path
+
+import pytest
+
+ROOT = Path(__file__).resolve().parent.parent
+
+
+def _free_port() -> int:
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _worker(rank: int, world: int, port: int, out_dir: str) -> None:
+    os.environ.update({"MASTER_ADDR": "127.0.0.1", "MASTER_PORT": str(port), "RANK": str(rank),
+                       "LOCAL_RANK": str(rank), "WORLD_SIZE": str(world), "SADCS_DIST_BACKEND": "gloo"})
+    sys.path.insert(0, str(ROOT))
+    import bench
+    import torch.distributed as dist
+
+    w, r, local = bench.dist_setup(world)
+    try:
+        bench.barrier(w)
+        result = {
+            "world": w, "rank": r, "local": local,
+            # a slower rank 1: the job's time is the max over ranks
+            "max": bench.max_over_ranks(10.0 + 5.0 * r, w),
+            # each rank processed its own text of (r + 1) MiB
+            "sum": bench.sum_over_ranks(float((r + 1) << 20), w),
+            "seed": bench.rank_seed(4, r),
+        }
+        bench.barrier(w)
+    finally:
+        dist.destroy_process_group()
+    Path(out_dir, f"rank{r}.json").write_text(json.dumps(result))
+
+
+def test_two_ranks_reduce_and_seed(tmp_path):
+    import torch.multiprocessing as mp
+
+    world = 2
+    port = _free_port()
+    mp.start_processes(_worker, args=(world, port, str(tmp_path)), nprocs=world, start_method="spawn", join=True)
+    results = [json.loads((tmp_path / f"rank{r}.json").read_text()) for r in range(world)]
+    for r, res in enumerate(results):
+        assert (res["world"], res["rank"], res["local"]) == (2, r, r)
+        assert res["max"] == 15.0
+        assert res["sum"] == float(3 << 20)
+    # every rank builds its own synthetic batch / request stream
+    assert results[0]["seed"] != results[1]["seed"]
+    assert results[0]["seed"] == 4  # rank 0 keeps the single-GPU workload
+
+
+def test_reference_arm_other_ranks_exit_without_work():
+    """--impl reference under a launcher: rank 1 prints nothing, does no work, exits 0, joins no group."""
+    env = dict(os.environ, RANK="1", LOCAL_RANK="1", WORLD_SIZE="2", MASTER_ADDR="127.0.0.1", MASTER_PORT="1")
+    proc = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--impl", "reference", "--gpus", "2",
+                           "--steps", "1", "--warmup", "0"], env=env, capture_output=True, text=True, timeout=120)
+    assert proc.returncode == 0, proc.stderr
+    assert proc.stdout.strip() == ""
+
+
+@pytest.mark.parametrize("workload", ["batch4096", "serve"])
+def test_reference_arm_unavailable_lines(workload):
+    proc = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--impl", "reference", "--workload", workload],
+                          capture_output=True, text=True, timeout=120)
+    assert proc.returncode == 0, proc.stderr
+    line = json.loads(proc.stdout.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and "unavailable" in line
