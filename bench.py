@@ -182,8 +182,17 @@ def sum_over_ranks(value: float, world: int) -> float:
 
 
 def rank_seed(base: int, rank: int) -> int:
-    """Seed of a rank's own synthetic batch or request stream (weak scaling: each rank its own)."""
+    """Seed of a rank's own synthetic request stream (weak scaling: each rank its own)."""
     return base + 1000 * rank
+
+
+def batch_share(count_per_rank: int, world: int, rank: int) -> list[int]:
+    """This rank's texts of one batch of count_per_rank * world texts, partitioned across ranks by
+    construction footprint (greedy longest-first); no data crosses between GPUs."""
+    from sadcs_b200 import workloads as W
+
+    lengths = W.batch_lengths(count_per_rank * world, lo=1 << 10, hi=4 << 20, seed=4)
+    return W.partition_by_footprint(lengths, world)[rank]
 
 
 # ---- CPU baseline (the reference's own CPU variant, or the oracle port) ----------------------------
@@ -446,7 +455,8 @@ def run_batch(args, world, rank, local) -> None:
     from sadcs_b200 import workloads as W
 
     torch.cuda.set_device(local)
-    texts = W.batch_texts(args.batch_count, lo=1 << 10, hi=4 << 20, seed=rank_seed(4, rank))
+    texts = W.batch_texts(args.batch_count * world, lo=1 << 10, hi=4 << 20, seed=4,
+                          indices=batch_share(args.batch_count, world, rank))
     lengths = [len(t) for t in texts]
     total = sum(lengths)
     packed = torch.from_numpy(np.concatenate(texts)).to(f"cuda:{local}")
@@ -479,6 +489,7 @@ def run_batch(args, world, rank, local) -> None:
     ms = start.elapsed_time(stop) / args.steps
     ms_max = max_over_ranks(ms, world)
     value = sum_over_ranks(float(total), world) / MIB / (ms_max / 1e3)
+    texts_total = sum_over_ranks(float(len(texts)), world)
 
     # The plain path: one construction per text (a bounded sample of the same texts), device-resident.
     sample = texts[:: max(1, len(texts) // args.plain_sample)][: args.plain_sample]
@@ -503,8 +514,10 @@ def run_batch(args, world, rank, local) -> None:
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_max, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
             "config": {"workload": "batch4096", "description": BATCH_DESC, "texts": len(texts), "total_bytes": total,
-                       "l2": "inputs larger than L2", "parallelism": "independent batches per GPU"},
-            "texts_per_s": round(len(texts) * world / (ms_max / 1e3), 1),
+                       "l2": "inputs larger than L2",
+                       "parallelism": ("one batch of %d texts per GPU, partitioned by footprint (longest first)"
+                                       % args.batch_count) if world > 1 else "single GPU"},
+            "texts_per_s": round(texts_total / (ms_max / 1e3), 1),
             "plain_one_text_per_launch": {"value": round(plain, 3), "unit": UNIT, "texts": len(sample),
                                           "texts_per_s": round(len(sample) / (plain_ms / 1e3), 1)},
             "speedup_vs_plain": round(value / world / plain, 2), "clocks": clocks, "gpu_launches": launches,

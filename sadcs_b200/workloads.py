@@ -198,17 +198,41 @@ def protein_text(rng: np.random.Generator, n: int) -> np.ndarray:
     return _AMINO[np.searchsorted(np.cumsum(p), rng.random(n), side="right").clip(0, 19)]
 
 
-def batch_texts(count: int = 4096, lo: int = 1 << 10, hi: int = 4 << 20, seed: int = 4):
-    """``count`` texts, lengths log-uniform in [lo, hi]; thirds over DNA, protein-like, uniform bytes."""
+def batch_lengths(count: int = 4096, lo: int = 1 << 10, hi: int = 4 << 20, seed: int = 4) -> np.ndarray:
+    """Lengths of a batch: log-uniform in [lo, hi]."""
     rng = np.random.default_rng(seed)
-    lengths = np.exp(rng.uniform(np.log(lo), np.log(hi), count)).astype(np.int64)
-    texts = []
-    for i, n in enumerate(lengths):
-        kind = i % 3
-        if kind == 0:
-            texts.append(_DNA[rng.integers(0, 4, int(n))])
-        elif kind == 1:
-            texts.append(protein_text(rng, int(n)))
-        else:
-            texts.append(rng.integers(0, 256, int(n), dtype=np.uint8))
-    return texts
+    return np.exp(rng.uniform(np.log(lo), np.log(hi), count)).astype(np.int64)
+
+
+def batch_text(index: int, n: int, seed: int = 4) -> np.ndarray:
+    """Text ``index`` of a batch (its own generator, so any subset can be made alone): DNA,
+    protein-like and uniform bytes by index mod 3."""
+    rng = np.random.default_rng([seed, index])
+    kind = index % 3
+    if kind == 0:
+        return _DNA[rng.integers(0, 4, int(n))]
+    if kind == 1:
+        return protein_text(rng, int(n))
+    return rng.integers(0, 256, int(n), dtype=np.uint8)
+
+
+def batch_texts(count: int = 4096, lo: int = 1 << 10, hi: int = 4 << 20, seed: int = 4, indices=None):
+    """``count`` texts, lengths log-uniform in [lo, hi]; thirds over DNA, protein-like, uniform bytes.
+    ``indices`` picks a subset (in the given order)."""
+    lengths = batch_lengths(count, lo, hi, seed)
+    picked = range(count) if indices is None else indices
+    return [batch_text(i, int(lengths[i]), seed) for i in picked]
+
+
+def partition_by_footprint(lengths, parts: int) -> list[list[int]]:
+    """Greedy longest-first bin packing of texts onto ``parts`` devices by construction footprint
+    (proportional to length): each text, longest first, goes to the least-loaded part. Every index
+    lands in exactly one part; each part keeps its indices in ascending order."""
+    order = sorted(range(len(lengths)), key=lambda i: (-int(lengths[i]), i))
+    loads = [0] * parts
+    out: list[list[int]] = [[] for _ in range(parts)]
+    for i in order:
+        k = min(range(parts), key=lambda q: (loads[q], q))
+        out[k].append(i)
+        loads[k] += int(lengths[i])
+    return [sorted(x) for x in out]

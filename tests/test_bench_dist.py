@@ -39,6 +39,7 @@ def _worker(rank: int, world: int, port: int, out_dir: str) -> None:
             # each rank processed its own text of (r + 1) MiB
             "sum": bench.sum_over_ranks(float((r + 1) << 20), w),
             "seed": bench.rank_seed(4, r),
+            "share": bench.batch_share(64, w, r),
         }
         bench.barrier(w)
     finally:
@@ -60,6 +61,30 @@ def test_two_ranks_reduce_and_seed(tmp_path):
     # every rank builds its own synthetic batch / request stream
     assert results[0]["seed"] != results[1]["seed"]
     assert results[0]["seed"] == 4  # rank 0 keeps the single-GPU workload
+    # one batch of 128 texts split across the two ranks: every text once, loads balanced
+    from sadcs_b200 import workloads as W
+
+    shares = [res["share"] for res in results]
+    assert sorted(shares[0] + shares[1]) == list(range(128))
+    lengths = W.batch_lengths(128, lo=1 << 10, hi=4 << 20, seed=4)
+    loads = [int(sum(lengths[i] for i in share)) for share in shares]
+    assert abs(loads[0] - loads[1]) <= int(lengths.max())
+
+
+def test_partition_by_footprint():
+    from sadcs_b200 import workloads as W
+
+    lengths = [5, 1, 9, 3, 3, 7, 2, 8]
+    parts = W.partition_by_footprint(lengths, 3)
+    assert sorted(sum(parts, [])) == list(range(8))
+    assert all(p == sorted(p) for p in parts)
+    loads = sorted(sum(lengths[i] for i in p) for p in parts)
+    assert loads == [12, 13, 13]  # longest first onto the least-loaded part
+    assert W.partition_by_footprint(lengths, 1) == [list(range(8))]
+    # a subset of a batch is generated identically on its own
+    full = W.batch_texts(9, lo=1 << 10, hi=1 << 12, seed=4)
+    part = W.batch_texts(9, lo=1 << 10, hi=1 << 12, seed=4, indices=[7, 2])
+    assert (part[0] == full[7]).all() and (part[1] == full[2]).all()
 
 
 def test_reference_arm_other_ranks_exit_without_work():
