@@ -22,13 +22,15 @@ constexpr int kClasses = 7;   // distance to the next sample position: 0 (the sa
 constexpr uint32_t kTextPad = 128;
 constexpr uint32_t kRankPad = 16;  // zero rank entries past the sample: a 7-rank window at any p <= n stays inside
 
-struct Cover {
+// The square tables come first and 16-byte aligned: kernels copy them to shared memory as words.
+struct alignas(16) Cover {
+    alignas(16) uint8_t tie[kV][kV];   // smallest k with a + k and b + k both sampled
+    alignas(16) uint8_t slot[kV][kV];  // [a][k]: index of sample a + k among the samples in [a, a + 32)
+    uint8_t below[kV];                 // cover residues below r
+    uint8_t classOf[kV];               // distance from residue r to the next cover residue
     uint8_t residue[kK];
-    uint8_t below[kV];           // cover residues below r
-    uint8_t classOf[kV];         // distance from residue r to the next cover residue
-    uint8_t tie[kV][kV];         // smallest k with a + k and b + k both sampled
-    uint8_t slot[kV][kV];        // [a][k]: index of sample a + k among the samples in [a, a + 32)
 };
+static_assert(offsetof(Cover, tie) % 16 == 0 && offsetof(Cover, slot) % 16 == 0, "word copies of the tables");
 
 constexpr bool coverHas(int r) {
     constexpr int d[kK] = {0, 1, 3, 8, 12, 19, 25};
