@@ -1,7 +1,8 @@
 """bench.py - suffix array + BWT construction throughput on B200, and the reference CPU arm.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--workload natural256m|uniform8m|genome3g]
-    python bench.py --impl reference ...
+    python bench.py --impl reference ...       the reference's CPU variant on the host cores
+    python bench.py --impl reference-gpu ...   the reference's own CUDA build on this GPU
 
 One step = one construction of the SA (uint32) and BWT of the workload's text, produced together.
 ``value`` is device throughput with the text resident in HBM (CUDA events on the stream the library
@@ -267,6 +268,77 @@ def run_reference(args, world, rank) -> None:
                                        f"{'reference CPU build (cover 128)' if kind == 'reference' else 'oracle port'}"},
             "e2e": {"value": round(value, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def run_reference_gpu(args, world, rank) -> None:
+    """--impl reference-gpu: the reference's own CUDA build (oracle/_ref/libsadcs_ref_gpu.so, its
+    gpusa.cu compiled unchanged for sm_100a) on this GPU, as its CLI's `bench --context --pinned`
+    measures it: page-locked host buffers, one context, gpuSuffixArray then gpuBwt per step (the
+    reference builds SA and BWT in two constructions), host to host. Rank 0 only."""
+    if rank != 0:
+        return
+    import ctypes
+
+    import oracle
+    from sadcs_b200 import workloads as W
+
+    desc, gen = WORKLOADS[args.workload]
+    base = {"impl": "reference-gpu", "metric": METRIC, "unit": UNIT}
+    if not oracle.ref_gpu_available():
+        print(json.dumps({**base, "unavailable": "oracle/_ref/libsadcs_ref_gpu.so not built (make -C oracle ref-gpu "
+                                                 "needs the reference sources)"}), flush=True)
+        return
+    text = gen(W)
+    n = int(len(text))
+    if n > (1 << 31) - 1025:
+        print(json.dumps({**base, "unavailable": "the reference's GPU API takes int32 sizes up to 2^31 - 1025 bytes"}),
+              flush=True)
+        return
+    try:
+        ctx = oracle.RefGpuContext(n)
+    except RuntimeError as e:
+        print(json.dumps({**base, "unavailable": str(e)}), flush=True)
+        return
+    h_text = oracle.ref_gpu_pinned(n)
+    h_sa = oracle.ref_gpu_pinned(4 * n)
+    h_bwt = oracle.ref_gpu_pinned(n)
+    try:
+        h_text[:] = text
+        sa_view = h_sa.view(np.int32)
+
+        def step():
+            _, sa_dev = ctx.suffix_array(h_text, out=sa_view)
+            _, primary, bwt_dev = ctx.bwt(h_text, out=h_bwt)
+            return sa_dev + bwt_dev, primary
+
+        for _ in range(max(args.warmup, 0)):
+            step()
+        host, device = [], []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            dev, primary = step()
+            host.append(time.perf_counter() - t0)
+            device.append(dev)
+        mean_host = sum(host) / len(host)
+        mean_dev = sum(device) / len(device)
+        value = n / MIB / mean_host
+        print(json.dumps({
+            **base, "value": round(value, 3), "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(mean_host * 1e3, 3), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+            "config": {"workload": args.workload, "description": desc, "text_bytes": n,
+                       "outputs": "SA (int32) by gpuSuffixArray, then BWT by gpuBwt (two constructions)",
+                       "cover": "mod 32 (the reference's GPU cover)", "build": "reference gpusa.cu, nvcc 12.9, sm_100a"},
+            "device_value": round(n / MIB / mean_dev, 3),
+            "device_ms_per_step": round(mean_dev * 1e3, 3),
+            "e2e": {"value": round(value, 3), "unit": UNIT, "h2d_bytes_per_step": 2 * n, "d2h_bytes_per_step": 5 * n,
+                    "api": "gpuSuffixArray + gpuBwt with a context and page-locked buffers"},
+        }), flush=True)
+    finally:
+        ctx.close()
+        for a in (h_text, h_sa, h_bwt):
+            if a is not None:
+                oracle.ref_gpu_free_pinned(a)
 
 
 # ---- our arm --------------------------------------------------------------------------------------
@@ -619,7 +691,7 @@ def main() -> None:
     p.add_argument("--gpus", type=int, default=1)
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
-    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--impl", choices=["ours", "reference", "reference-gpu"], default="ours")
     p.add_argument("--workload", choices=sorted(WORKLOADS) + ["batch4096", "serve"], default="natural256m")
     p.add_argument("--batch-count", type=int, default=4096)
     p.add_argument("--plain-sample", type=int, default=64)
@@ -633,6 +705,10 @@ def main() -> None:
     p.add_argument("--no-e2e", dest="e2e", action="store_false")
     p.add_argument("--no-verify", dest="verify", action="store_false")
     args = p.parse_args()
+    if args.impl == "reference-gpu":
+        world, rank, _ = rank_env()
+        run_reference_gpu(args, world, rank)
+        return
     if args.impl == "reference":
         # Rank 0 alone times the reference on the host cores; other ranks exit without work (and
         # without joining a process group, so nothing waits on them).

@@ -12,6 +12,9 @@ Two libraries:
 * ``_ref/libsadcs_ref.so`` - the reference's own CPU variant (src/cpu, src/common of acesds/sadcs),
   compiled from its sources by ``make -C oracle ref`` where they exist. Optional at run time: it is
   not committed (the sources are not ours) and is absent wherever it was not built.
+* ``_ref/libsadcs_ref_gpu.so`` - the reference's own CUDA variant (src/cuda/gpusa.cu) for sm_100a,
+  by ``make -C oracle ref-gpu``: the reference's GPU construction on the same device, for the
+  timed comparison in bench.py and as a second parity source in the GPU tests.
 """
 from __future__ import annotations
 
@@ -26,6 +29,7 @@ HERE = Path(__file__).resolve().parent
 ORACLE_SO = HERE / "liboracle.so"
 REF_SO = HERE / "_ref" / "libsadcs_ref.so"
 REF_CLI = HERE / "_ref" / "sadcs_ref"
+REF_GPU_SO = HERE / "_ref" / "libsadcs_ref_gpu.so"
 
 _u8p = ctypes.POINTER(ctypes.c_uint8)
 _u32p = ctypes.POINTER(ctypes.c_uint32)
@@ -34,6 +38,7 @@ _i64p = ctypes.POINTER(ctypes.c_int64)
 
 _lib = None
 _ref = None
+_ref_gpu = None
 
 
 def build(quiet: bool = True) -> None:
@@ -104,6 +109,91 @@ def ref() -> ctypes.CDLL:
         L.ref_max_text_size.restype = ctypes.c_longlong
         _ref = L
     return _ref
+
+
+def ref_gpu_available() -> bool:
+    return REF_GPU_SO.exists()
+
+
+def ref_gpu() -> ctypes.CDLL:
+    """The reference's own CUDA build; raises if it was not built."""
+    global _ref_gpu
+    if _ref_gpu is None:
+        if not REF_GPU_SO.exists():
+            raise FileNotFoundError(f"{REF_GPU_SO} not built (make -C oracle ref-gpu, needs the reference sources)")
+        L = ctypes.CDLL(str(REF_GPU_SO))
+        L.ref_gpu_create_context.restype = ctypes.c_int
+        L.ref_gpu_create_context.argtypes = [ctypes.c_int32, ctypes.POINTER(ctypes.c_void_p)]
+        L.ref_gpu_destroy_context.restype = None
+        L.ref_gpu_destroy_context.argtypes = [ctypes.c_void_p]
+        L.ref_gpu_suffix_array.restype = ctypes.c_int
+        L.ref_gpu_suffix_array.argtypes = [ctypes.c_void_p, _u8p, ctypes.c_int32, _i32p,
+                                           ctypes.POINTER(ctypes.c_double)]
+        L.ref_gpu_bwt.restype = ctypes.c_int
+        L.ref_gpu_bwt.argtypes = [ctypes.c_void_p, _u8p, ctypes.c_int32, _u8p, _i32p, ctypes.POINTER(ctypes.c_double)]
+        L.ref_gpu_allocate_pinned.restype = ctypes.c_void_p
+        L.ref_gpu_allocate_pinned.argtypes = [ctypes.c_size_t]
+        L.ref_gpu_free_pinned.restype = None
+        L.ref_gpu_free_pinned.argtypes = [ctypes.c_void_p]
+        L.ref_gpu_last_error.restype = ctypes.c_char_p
+        _ref_gpu = L
+    return _ref_gpu
+
+
+class RefGpuContext:
+    """A context of the reference's CUDA build (gpuCreateContext) for texts of up to capacity bytes."""
+
+    def __init__(self, capacity: int):
+        L = ref_gpu()
+        self.handle = ctypes.c_void_p()
+        status = L.ref_gpu_create_context(int(capacity), ctypes.byref(self.handle))
+        if status != 0:
+            raise RuntimeError(f"reference gpuCreateContext: status {status}: {L.ref_gpu_last_error().decode()}")
+
+    def suffix_array(self, text: np.ndarray, out: np.ndarray | None = None) -> tuple[np.ndarray, float]:
+        """(SA, device seconds) of the reference's GPU construction."""
+        L = ref_gpu()
+        t = _text(text)
+        n = len(t)
+        sa = out if out is not None else np.zeros(max(n, 1), np.int32)
+        seconds = ctypes.c_double(0)
+        status = L.ref_gpu_suffix_array(self.handle, _ptr(_nonempty(t), _u8p), n, _ptr(sa, _i32p),
+                                        ctypes.byref(seconds))
+        if status != 0:
+            raise RuntimeError(f"reference gpuSuffixArray: status {status}: {L.ref_gpu_last_error().decode()}")
+        return sa[:n], seconds.value
+
+    def bwt(self, text: np.ndarray, out: np.ndarray | None = None) -> tuple[np.ndarray, int, float]:
+        """(BWT, primary, device seconds) of the reference's GPU construction."""
+        L = ref_gpu()
+        t = _text(text)
+        n = len(t)
+        bwt = out if out is not None else np.zeros(max(n, 1), np.uint8)
+        primary = ctypes.c_int32(0)
+        seconds = ctypes.c_double(0)
+        status = L.ref_gpu_bwt(self.handle, _ptr(_nonempty(t), _u8p), n, _ptr(bwt, _u8p), ctypes.byref(primary),
+                               ctypes.byref(seconds))
+        if status != 0:
+            raise RuntimeError(f"reference gpuBwt: status {status}: {L.ref_gpu_last_error().decode()}")
+        return bwt[:n], int(primary.value), seconds.value
+
+    def close(self) -> None:
+        if self.handle:
+            ref_gpu().ref_gpu_destroy_context(self.handle)
+            self.handle = ctypes.c_void_p()
+
+
+def ref_gpu_pinned(nbytes: int) -> np.ndarray | None:
+    """Page-locked host memory from the reference's gpuAllocatePinned (None if unavailable); free
+    with ref_gpu_free_pinned."""
+    p = ref_gpu().ref_gpu_allocate_pinned(int(nbytes))
+    if not p:
+        return None
+    return np.ctypeslib.as_array(ctypes.cast(p, ctypes.POINTER(ctypes.c_uint8)), shape=(int(nbytes),))
+
+
+def ref_gpu_free_pinned(a: np.ndarray) -> None:
+    ref_gpu().ref_gpu_free_pinned(ctypes.c_void_p(a.ctypes.data))
 
 
 def _ptr(a: np.ndarray, t):
