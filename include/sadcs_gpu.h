@@ -167,6 +167,27 @@ int sadcs_gpu_build_batch_device(sadcs_gpu_context* context, const uint8_t* d_te
 int sadcs_gpu_check_suffix_array(const uint8_t* d_text, int64_t n, const uint32_t* d_sa, int64_t* bad_index,
                                  const char** reason, void* stream);
 
+/* No counterpart in the reference (its checker is CPU code that allocates host memory): the check
+ * of sadcs_gpu_check_suffix_array, same arguments and results, allocating nothing - no device
+ * memory, no page-locked host memory, no library routine that allocates. It is for callers that
+ * must not allocate: code running beside a serving loop (sadcs_gpu_server_*) whose memory budget is
+ * already promised to admitted constructions, where a new allocation could fail or take memory a
+ * construction was admitted against; and code on a latency-critical path, where page-locking host
+ * memory and growing a stream-ordered pool cost time and can fail.
+ * Its scratch is one fixed array in the library's device code (4 MiB: the inverse suffix array of
+ * up to SADCS_GPU_STATIC_CHECK_MAX entries, plus three result words). n above that limit is rejected
+ * with SADCS_FAILED and a message naming the limit; nothing is launched.
+ * The first call on each device looks up the array's address (cudaGetSymbolAddress), which may load
+ * the library's device code: make that first call before capturing any stream.
+ * Initial values: each call sets its three result words itself (to all ones) before its kernels
+ * run; the inverse-suffix-array words need none (every word the verdict depends on is written by
+ * the same call).
+ * All calls on one device share that one array: calls that overlap in time (on other streams or
+ * from other threads) race on it and their verdicts are undefined - serialise them. */
+#define SADCS_GPU_STATIC_CHECK_MAX 1048576
+int sadcs_gpu_check_suffix_array_static(const uint8_t* d_text, int64_t n, const uint32_t* d_sa,
+                                        int64_t* bad_index, const char** reason, void* stream);
+
 /* ---- serving (no counterpart) --------------------------------------------------------------------
  * A request loop on the current device: requests are submitted at any time and complete
  * asynchronously; queued small requests (up to small_limit bytes) are merged into one batched

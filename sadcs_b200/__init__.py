@@ -157,6 +157,9 @@ def lib() -> ctypes.CDLL:
         L.sadcs_gpu_check_suffix_array.restype = ctypes.c_int
         L.sadcs_gpu_check_suffix_array.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, _i64p,
                                                    ctypes.POINTER(ctypes.c_char_p), ctypes.c_void_p]
+        L.sadcs_gpu_check_suffix_array_static.restype = ctypes.c_int
+        L.sadcs_gpu_check_suffix_array_static.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, _i64p,
+                                                          ctypes.POINTER(ctypes.c_char_p), ctypes.c_void_p]
         _lib = L
     return _lib
 
@@ -364,6 +367,20 @@ def check_suffix_array_device(d_text: int, n: int, d_sa: int, stream: int | None
     _check(lib().sadcs_gpu_check_suffix_array(ctypes.c_void_p(d_text), int(n), ctypes.c_void_p(d_sa),
                                               ctypes.byref(index), ctypes.byref(reason),
                                               ctypes.c_void_p(stream) if stream else None))
+    return index.value < 0, int(index.value), reason.value.decode() if reason.value else None
+
+
+STATIC_CHECK_MAX = 1 << 20  # SADCS_GPU_STATIC_CHECK_MAX
+
+
+def check_suffix_array_static_device(d_text: int, n: int, d_sa: int, stream: int | None = None):
+    """check_suffix_array_device without any allocation (sadcs_gpu_check_suffix_array_static): n up
+    to STATIC_CHECK_MAX; calls on one device must not overlap in time."""
+    index = ctypes.c_int64(-1)
+    reason = ctypes.c_char_p()
+    _check(lib().sadcs_gpu_check_suffix_array_static(ctypes.c_void_p(d_text), int(n), ctypes.c_void_p(d_sa),
+                                                     ctypes.byref(index), ctypes.byref(reason),
+                                                     ctypes.c_void_p(stream) if stream else None))
     return index.value < 0, int(index.value), reason.value.decode() if reason.value else None
 
 

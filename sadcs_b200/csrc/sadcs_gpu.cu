@@ -14,6 +14,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -947,6 +948,91 @@ int sadcs_gpu_check_suffix_array(const uint8_t* d_text, int64_t n, const uint32_
     cudaStreamSynchronize(st);
     cudaFreeHost(host);
     if (error != cudaSuccess) return failed("suffix array check", error);
+    if (bad_index) *bad_index = index;
+    if (reason) *reason = why;
+    return SADCS_OK;
+}
+
+// ---- the suffix array check without allocation ------------------------------------------------
+
+namespace {
+
+// Scratch of sadcs_gpu_check_suffix_array_static, in module memory: three 64-bit result words at
+// word 0 (set to all ones by every call), the inverse suffix array from word 64 (no initial value
+// needed: each word a verdict reads is written by the same call's scatter). Shared by every call on
+// a device, so overlapping calls race.
+constexpr int64_t kStaticCheckMax = SADCS_GPU_STATIC_CHECK_MAX;
+constexpr size_t kStaticCheckIsaWord = 64;
+static __device__ __align__(256) uint32_t gStaticCheckScratch[kStaticCheckIsaWord + kStaticCheckMax];
+
+constexpr int kStaticCheckDevices = 64;
+std::mutex gStaticCheckLock;
+uint32_t* gStaticCheckAddress[kStaticCheckDevices] = {};
+
+// The scratch's device address on the current device, looked up on the first call per device.
+cudaError_t staticCheckScratch(uint32_t** out) {
+    int device = 0;
+    cudaError_t error = cudaGetDevice(&device);
+    if (error != cudaSuccess) return error;
+    if (device < 0 || device >= kStaticCheckDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> hold(gStaticCheckLock);
+    if (!gStaticCheckAddress[device]) {
+        void* address = nullptr;
+        if ((error = cudaGetSymbolAddress(&address, gStaticCheckScratch)) != cudaSuccess) return error;
+        gStaticCheckAddress[device] = static_cast<uint32_t*>(address);
+    }
+    *out = gStaticCheckAddress[device];
+    return cudaSuccess;
+}
+
+}  // namespace
+
+int sadcs_gpu_check_suffix_array_static(const uint8_t* d_text, int64_t n, const uint32_t* d_sa, int64_t* bad_index,
+                                        const char** reason, void* stream) {
+    tLastError[0] = '\0';
+    if (bad_index) *bad_index = -1;
+    if (reason) *reason = nullptr;
+    if (n <= 0) return SADCS_OK;
+    if (n > kStaticCheckMax) {
+        setError("text of %lld bytes exceeds the %lld entries of the static scratch of "
+                 "sadcs_gpu_check_suffix_array_static (sadcs_gpu_check_suffix_array has no such limit)",
+                 static_cast<long long>(n), static_cast<long long>(kStaticCheckMax));
+        return SADCS_FAILED;
+    }
+    uint32_t* scratch = nullptr;
+    cudaError_t error = staticCheckScratch(&scratch);
+    if (error != cudaSuccess) return failed("cudaGetSymbolAddress of the static check scratch", error);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const uint32_t count = static_cast<uint32_t>(n);
+    unsigned long long* words = reinterpret_cast<unsigned long long*>(scratch);
+    uint32_t* isa = scratch + kStaticCheckIsaWord;
+    unsigned long long host[3] = {kNoFailure, kNoFailure, kNoFailure};  // pageable: nothing is allocated
+    const uint32_t blocks = (count + 255) / 256;
+    error = cudaMemsetAsync(words, 0xFF, 3 * sizeof(unsigned long long), st);
+    if (error == cudaSuccess) error = launch(checkScatter, blocks, 256, 0, st, d_sa, count, isa, words);
+    if (error == cudaSuccess) error = cudaMemcpyAsync(host, words, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
+    if (error == cudaSuccess) error = cudaStreamSynchronize(st);
+    const char* why = nullptr;
+    int64_t index = -1;
+    if (error == cudaSuccess && host[0] != kNoFailure) {
+        why = "entry out of range";
+        index = static_cast<int64_t>(host[0]);
+    }
+    if (error == cudaSuccess && !why) {
+        error = launch(checkDuplicates, blocks, 256, 0, st, d_sa, count, isa, words + 1);
+        if (error == cudaSuccess) error = launch(checkOrder, blocks, 256, 0, st, d_text, d_sa, count, isa, words + 2);
+        if (error == cudaSuccess)
+            error = cudaMemcpyAsync(host + 1, words + 1, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
+        if (error == cudaSuccess) error = cudaStreamSynchronize(st);
+        if (error == cudaSuccess && host[1] != kNoFailure) {
+            why = "duplicate entry";
+            index = static_cast<int64_t>(host[1]);
+        } else if (error == cudaSuccess && host[2] != kNoFailure) {
+            why = "SA[index] and SA[index + 1] out of order";
+            index = static_cast<int64_t>(host[2]);
+        }
+    }
+    if (error != cudaSuccess) return failed("suffix array check (static scratch)", error);
     if (bad_index) *bad_index = index;
     if (reason) *reason = why;
     return SADCS_OK;
