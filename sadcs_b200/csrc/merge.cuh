@@ -30,7 +30,7 @@
 namespace sadcs {
 
 constexpr uint32_t kMergeG = 32;
-constexpr uint32_t kMergeR = 32;
+constexpr uint32_t kMergeR = 30;  // with G = 32: tiles of at most 1147 records
 constexpr uint32_t kMergeCap = kMergeG * kMergeR + 6 * (kMergeG - 1) + 1;
 constexpr int kMergeThreads = 256;
 constexpr int kPairs = kClasses * (kClasses - 1) / 2;
@@ -194,7 +194,59 @@ __device__ __forceinline__ int listOfElement(const uint32_t* seg, uint32_t e) {
     return l;
 }
 
-template <bool kFinal>
+// Thread 0 of a tile: its window in every list (t.win, t.seg), the number of elements before the
+// windows (t.base), the window indices of the tile's two splitters (t.loIdx, t.hiIdx; kNoList for
+// the ends of the level) and whether the window set fits (t.bad otherwise, never by construction).
+__device__ __forceinline__ void planTileWindows(const MergeArgs& a, MergeTileInfo& t) {
+    const uint32_t* st = a.level.start;
+    uint32_t w[kClasses], e[kClasses];
+    uint32_t loList = kNoList, hiList = kNoList;
+    if (!a.rowsIn) {
+        for (int b = 0; b < kClasses; b++) {
+            w[b] = 0;
+            e[b] = st[b + 1] - st[b];
+        }
+    } else {
+        const MergeRow lo = a.rowsIn[blockIdx.x];
+        const MergeRow hi = a.rowsIn[blockIdx.x + 1];
+        loList = lo.list;
+        hiList = hi.list;
+        for (int b = 0; b < kClasses; b++) {
+            const uint32_t len = st[b + 1] - st[b];
+            if (lo.list == kNoList) {
+                w[b] = 0;
+            } else if (static_cast<uint32_t>(b) == lo.list) {
+                w[b] = lo.c[b] * kMergeG;
+            } else {
+                w[b] = lo.c[b] == 0 ? 0 : (lo.c[b] - 1) * kMergeG + 1;
+            }
+            if (hi.list == kNoList) {
+                e[b] = len;
+            } else if (static_cast<uint32_t>(b) == hi.list) {
+                e[b] = hi.c[b] * kMergeG + 1;
+            } else {
+                e[b] = min(len, hi.c[b] * kMergeG);
+            }
+            w[b] = min(w[b], len);
+            e[b] = max(min(e[b], len), w[b]);
+        }
+    }
+    uint32_t base = 0;
+    t.seg[0] = 0;
+    for (int b = 0; b < kClasses; b++) {
+        t.win[b] = w[b];
+        t.seg[b + 1] = t.seg[b] + (e[b] - w[b]);
+        base += w[b];
+    }
+    t.base = base;
+    t.size = t.seg[kClasses];
+    t.loIdx = loList == kNoList ? kNoList : t.seg[loList];
+    t.hiIdx = hiList == kNoList ? kNoList : t.seg[hiList + 1] - 1;
+    t.bad = t.size > kMergeCap;
+}
+
+// An upper level's tiles: the rows (every R-th element of the merged order with its per-list counts)
+// that bound the tiles of the level below.
 __global__ void __launch_bounds__(kMergeThreads) mergeTiles(MergeArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     MergeRecord* rec = reinterpret_cast<MergeRecord*>(smem);
@@ -212,51 +264,7 @@ __global__ void __launch_bounds__(kMergeThreads) mergeTiles(MergeArgs a) {
     }
 
     if (threadIdx.x == 0) {
-        const uint32_t* st = a.level.start;
-        uint32_t w[kClasses], e[kClasses];
-        uint32_t loList = kNoList, hiList = kNoList;
-        if (!a.rowsIn) {
-            for (int b = 0; b < kClasses; b++) {
-                w[b] = 0;
-                e[b] = st[b + 1] - st[b];
-            }
-        } else {
-            const MergeRow lo = a.rowsIn[blockIdx.x];
-            const MergeRow hi = a.rowsIn[blockIdx.x + 1];
-            loList = lo.list;
-            hiList = hi.list;
-            for (int b = 0; b < kClasses; b++) {
-                const uint32_t len = st[b + 1] - st[b];
-                if (lo.list == kNoList) {
-                    w[b] = 0;
-                } else if (static_cast<uint32_t>(b) == lo.list) {
-                    w[b] = lo.c[b] * kMergeG;
-                } else {
-                    w[b] = lo.c[b] == 0 ? 0 : (lo.c[b] - 1) * kMergeG + 1;
-                }
-                if (hi.list == kNoList) {
-                    e[b] = len;
-                } else if (static_cast<uint32_t>(b) == hi.list) {
-                    e[b] = hi.c[b] * kMergeG + 1;
-                } else {
-                    e[b] = min(len, hi.c[b] * kMergeG);
-                }
-                w[b] = min(w[b], len);
-                e[b] = max(min(e[b], len), w[b]);
-            }
-        }
-        uint32_t base = 0;
-        t.seg[0] = 0;
-        for (int b = 0; b < kClasses; b++) {
-            t.win[b] = w[b];
-            t.seg[b + 1] = t.seg[b] + (e[b] - w[b]);
-            base += w[b];
-        }
-        t.base = base;
-        t.size = t.seg[kClasses];
-        t.loIdx = loList == kNoList ? kNoList : t.seg[loList];
-        t.hiIdx = hiList == kNoList ? kNoList : t.seg[hiList + 1] - 1;
-        t.bad = t.size > kMergeCap;
+        planTileWindows(a, t);
         const uint32_t steps = (kClasses - 1) * t.size;
         const uint32_t lanes = kMergeThreads - kPairs;
         const uint32_t c = max(1u, (steps + lanes - 1) / lanes);
@@ -365,25 +373,15 @@ __global__ void __launch_bounds__(kMergeThreads) mergeTiles(MergeArgs a) {
             atomicExch(a.error, 2u);
             continue;
         }
-        if constexpr (kFinal) {
-            const uint32_t p = rec[e].pos, tj = rec[e].text;
-            const uint32_t first = a.texts.startOf(tj);
-            if (a.sa) a.sa[g] = p - first;
-            if (a.bwt && p != first) {
-                const uint32_t base = __ldg(a.outBase + tj), row = g - base, zero = __ldg(a.rowZero + tj);
-                a.bwt[base + (row < zero ? row + 1 : row)] = charByte(a.texts, p - 1);
-            }
-        } else {
-            if (g % kMergeR == 0) {
-                const int l = listOfElement(t.seg, e);
-                MergeRow row;
-                row.list = static_cast<uint32_t>(l);
+        if (g % kMergeR == 0) {
+            const int l = listOfElement(t.seg, e);
+            MergeRow row;
+            row.list = static_cast<uint32_t>(l);
 #pragma unroll
-                for (int b = 0; b < kClasses; b++) {
-                    row.c[b] = b == l ? t.win[l] + (e - t.seg[l]) : t.win[b] + cnt[e * 8 + b];
-                }
-                a.rowsOut[g / kMergeR] = row;
+            for (int b = 0; b < kClasses; b++) {
+                row.c[b] = b == l ? t.win[l] + (e - t.seg[l]) : t.win[b] + cnt[e * 8 + b];
             }
+            a.rowsOut[g / kMergeR] = row;
         }
     }
 }
@@ -481,6 +479,9 @@ inline MergePlan planMerge(const uint32_t* classStart) {
     return p;
 }
 
+// The final level (merge_final.cuh).
+inline cudaError_t launchFinal(const MergeArgs& args, uint32_t tiles, cudaStream_t stream);
+
 // Merges the class lists of the texts into sa and/or bwt (either may be null). splitters and rows
 // are scratch sized by planMerge; counter is one device word (scratch); rowZero and outBase are per
 // text (rowZero is filled here when a BWT is asked for); rowBase: the class tables' row bases.
@@ -493,9 +494,7 @@ inline cudaError_t mergeClasses(const uint8_t* text, const uint32_t* ranks, cons
     int device = 0;
     SADCS_TRY(cudaGetDevice(&device));
     if (!(configured >> (device & 63) & 1)) {
-        SADCS_TRY(cudaFuncSetAttribute(mergeTiles<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       static_cast<int>(mergeSharedBytes())));
-        SADCS_TRY(cudaFuncSetAttribute(mergeTiles<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        SADCS_TRY(cudaFuncSetAttribute(mergeTiles, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(mergeSharedBytes())));
         configured |= uint64_t(1) << (device & 63);
     }
@@ -533,13 +532,13 @@ inline cudaError_t mergeClasses(const uint8_t* text, const uint32_t* ranks, cons
             args.sa = sa;
             args.bwt = bwt;
             if (finalStart) SADCS_TRY(cudaEventRecord(finalStart, stream));
-            SADCS_TRY(launch(mergeTiles<true>, tiles, kMergeThreads, mergeSharedBytes(), stream, args));
+            SADCS_TRY(launchFinal(args, tiles, stream));
             if (finalStop) SADCS_TRY(cudaEventRecord(finalStop, stream));
         } else {
             args.rowsOut = rows + plan.rowIndex[L - 1];
             SADCS_TRY(launch(mergeWriteSentinel, 1, 32, 0, stream, rows + plan.rowIndex[L - 1] + plan.tiles[L - 1],
                              level[L]));
-            SADCS_TRY(launch(mergeTiles<false>, tiles, kMergeThreads, mergeSharedBytes(), stream, args));
+            SADCS_TRY(launch(mergeTiles, tiles, kMergeThreads, mergeSharedBytes(), stream, args));
         }
     }
     SADCS_TRY(cudaMemcpyAsync(hostWord, counter, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));

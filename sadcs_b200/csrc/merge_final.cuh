@@ -1,0 +1,285 @@
+// merge_final.cuh - the last merge level: every tile of the 7 class lists merged in shared memory and
+// written as the suffix array and the BWT.
+//
+// A tile's window set (at most kMergeCap records, merge.cuh) is held as arrays of fields, not as
+// records, so the 32 threads of a warp reading one field of 32 records hit 32 different banks:
+//   words[W][cap]  the code stream from the suffix's first character, W = ceil(31 * bits / 64)
+//                  64-bit words: every comparison reads k < 32 characters (k = the cover's tie
+//                  offset), so no comparison reads global memory
+//   rank[7][cap]   the 7 sample ranks of [p, p + 32)
+//   pos[cap]       p; end[cap] the end of p's text (several texts only)
+//   prev[cap]      the code of the character before p (the BWT byte)
+//   idxA, idxB     u16 orders of the records
+// The 7 windows are merged by a 3-level tree: (0,1) (2,3) (4,5) 6, then (01,23) (45,6), then
+// (0123,456). Each level splits its output into equal chunks, one per thread; a thread finds its
+// chunk's start on the merge path of its merge by binary search and walks it, writing record
+// indices. The final order gives every record's rank within the window set, hence its place in the
+// output (base + rank) for the records between the tile's two splitters.
+#pragma once
+
+#include "merge.cuh"
+
+namespace sadcs {
+
+// 64-bit words of the code stream a final-level record keeps: 31 characters of `bits` bits.
+__host__ __device__ constexpr int finalWords(uint32_t bits) {
+    return static_cast<int>((31 * bits + 63) / 64);
+}
+
+template <int W, bool kMulti>
+struct FinalTile {
+    static constexpr size_t kPerRecord = 8 * W + 4 * kK + 4 + (kMulti ? 4 : 0) + 2 + 2 + 1;
+    static constexpr size_t sharedBytes() { return kMergeCap * kPerRecord + 64; }
+    uint64_t* words;
+    uint32_t* rank;
+    uint32_t* pos;
+    uint32_t* end;
+    uint16_t* idxA;
+    uint16_t* idxB;
+    uint8_t* prev;
+    __device__ __forceinline__ void carve(unsigned char* smem) {
+        words = reinterpret_cast<uint64_t*>(smem);
+        rank = reinterpret_cast<uint32_t*>(words + W * kMergeCap);
+        pos = rank + kK * kMergeCap;
+        end = pos + kMergeCap;
+        idxA = reinterpret_cast<uint16_t*>(end + (kMulti ? kMergeCap : 0));
+        idxB = idxA + kMergeCap;
+        prev = reinterpret_cast<uint8_t*>(idxB + kMergeCap);
+    }
+};
+
+// Suffix x < suffix y (record indices of the tile), by the difference-cover comparison
+// (merge.cuh: lessRecord) on the shared-memory fields.
+template <int W, bool kMulti>
+__device__ __forceinline__ bool finalLess(const FinalTile<W, kMulti>& s, uint32_t x, uint32_t y, uint32_t n,
+                                          uint32_t bits, const MergeTables& tb) {
+    if constexpr (kMulti) {
+        const uint32_t ex = s.end[x], ey = s.end[y];
+        if (ex != ey) return ex < ey;  // different texts: text order
+        n = ex;
+    }
+    const uint32_t i = s.pos[x], j = s.pos[y];
+    const uint32_t k = tb.tie[i % kV][j % kV];
+    const uint32_t common = min(k, min(n - i, n - j));
+    const uint32_t cbits = common * bits;
+#pragma unroll
+    for (int w = 0; w < W; w++) {
+        if (cbits <= 64u * w) break;
+        uint64_t a = s.words[w * kMergeCap + x], b = s.words[w * kMergeCap + y];
+        if (cbits < 64u * (w + 1)) {
+            const uint64_t mk = ~uint64_t(0) << (64u * (w + 1) - cbits);
+            a &= mk;
+            b &= mk;
+        }
+        if (a != b) return a < b;
+    }
+    if (common < k || i + k == n || j + k == n) return i > j;  // one is a prefix of the other
+    return s.rank[tb.slot[i % kV][k] * kMergeCap + x] < s.rank[tb.slot[j % kV][k] * kMergeCap + y];
+}
+
+// One tree level: the merges m (A = [mb[3m], mb[3m + 1]), B = [mb[3m + 1], mb[3m + 2]) of src,
+// written to dst from mb[3m]), which together cover [0, size); mb is in shared memory. Thread t
+// writes outputs [t * chunk, (t + 1) * chunk).
+template <int W, bool kMulti>
+__device__ __forceinline__ void finalLevel(const FinalTile<W, kMulti>& s, const uint16_t* src, uint16_t* dst,
+                                           const uint32_t* mb, int merges, uint32_t size, uint32_t n, uint32_t bits,
+                                           const MergeTables& tb) {
+    const uint32_t chunk = (size + kMergeThreads - 1) / kMergeThreads;
+    uint32_t at = threadIdx.x * chunk;
+    const uint32_t stopAll = min(at + chunk, size);
+    int m = 0;
+    while (at < stopAll) {
+        while (m + 1 < merges && at >= mb[3 * m + 2]) m++;
+        const uint32_t a0 = mb[3 * m], a1 = mb[3 * m + 1], b1 = mb[3 * m + 2];
+        const uint32_t lenA = a1 - a0, lenB = b1 - a1;
+        uint32_t d = at - a0;
+        const uint32_t stop = min(stopAll, b1) - a0;
+        uint32_t lo = d > lenB ? d - lenB : 0, hi = min(d, lenA);
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (finalLess(s, src[a0 + mid], src[a1 + d - 1 - mid], n, bits, tb)) {
+                lo = mid + 1;
+            } else {
+                hi = mid;
+            }
+        }
+        uint32_t i = lo, j = d - lo;
+        uint32_t xa = i < lenA ? src[a0 + i] : 0, xb = j < lenB ? src[a1 + j] : 0;
+        for (; d < stop; d++) {
+            if (j == lenB || (i < lenA && finalLess(s, xa, xb, n, bits, tb))) {
+                dst[a0 + d] = static_cast<uint16_t>(xa);
+                i++;
+                if (i < lenA) xa = src[a0 + i];
+            } else {
+                dst[a0 + d] = static_cast<uint16_t>(xb);
+                j++;
+                if (j < lenB) xb = src[a1 + j];
+            }
+        }
+        at = a0 + stop;
+    }
+}
+
+template <int W, bool kMulti>
+__global__ void __launch_bounds__(kMergeThreads) mergeFinal(MergeArgs a) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    FinalTile<W, kMulti> s;
+    s.carve(smem);
+    __shared__ MergeTileInfo t;
+    __shared__ __align__(16) MergeTables tb;
+    __shared__ uint32_t sLo, sHi;
+    __shared__ uint32_t bounds[3 * 7];  // the tree's merges: 4 + 2 + 1 triples of window offsets
+    {
+        const uint32_t* src = reinterpret_cast<const uint32_t*>(&cCover.tie[0][0]);
+        uint32_t* dst = reinterpret_cast<uint32_t*>(&tb.tie[0][0]);
+        for (int i = threadIdx.x; i < kV * kV / 4; i += kMergeThreads) dst[i] = src[i];
+        const uint32_t* src2 = reinterpret_cast<const uint32_t*>(&cCover.slot[0][0]);
+        uint32_t* dst2 = reinterpret_cast<uint32_t*>(&tb.slot[0][0]);
+        for (int i = threadIdx.x; i < kV * kV / 4; i += kMergeThreads) dst2[i] = src2[i];
+    }
+    if (threadIdx.x == 0) {
+        planTileWindows(a, t);
+        sLo = 0;
+        sHi = t.size;
+        // (0,1) (2,3) (4,5) (6,-), then (01,23) (45,6), then (0123,456): indices into t.seg
+        constexpr uint8_t kTree[21] = {0, 1, 2, 2, 3, 4, 4, 5, 6, 6, 7, 7, 0, 2, 4, 4, 6, 7, 0, 4, 7};
+        for (int i = 0; i < 21; i++) bounds[i] = t.seg[kTree[i]];
+        if (t.bad && a.error) atomicExch(a.error, 1u);
+    }
+    __syncthreads();
+    if (t.bad) return;
+    const uint32_t size = t.size;
+    const uint32_t* st = a.level.start;
+    const uint32_t bits = a.texts.bits;
+    const uint32_t n = kMulti ? 0u : a.texts.oneEnd;
+
+    // Gather: positions from the lists (coalesced), then each record's code words and ranks by
+    // asynchronous copies, all in flight at once; the word after them and the word before them
+    // (when the previous character starts there) by plain loads, also in flight.
+    constexpr int kItems = (kMergeCap + kMergeThreads - 1) / kMergeThreads;
+    uint32_t p[kItems];
+    uint64_t extra[kItems], before[kItems];
+#pragma unroll
+    for (int j = 0; j < kItems; j++) {
+        const uint32_t e = threadIdx.x + j * kMergeThreads;
+        p[j] = 0;
+        if (e < size) {
+            const int l = listOfElement(t.seg, e);
+            uint32_t q = a.level.lists[st[l] + t.win[l] + (e - t.seg[l])];
+            const uint32_t qEnd = a.texts.endOf(q);
+            if (q >= qEnd) {  // cannot happen for valid class lists; never read out of range
+                atomicExch(a.error, 3u);
+                q = 0;
+            }
+            p[j] = q;
+            s.pos[e] = q;
+            if constexpr (kMulti) s.end[e] = q < qEnd ? qEnd : a.texts.endOf(0);
+            s.idxA[e] = static_cast<uint16_t>(e);
+            const uint64_t* src = a.texts.packed + ((static_cast<uint64_t>(q) * bits) >> 6);
+#pragma unroll
+            for (int w = 0; w < W; w++) cpAsync8(&s.words[w * kMergeCap + e], src + w);
+            const uint32_t* rk = a.ranks + pack(q);
+#pragma unroll
+            for (int r = 0; r < kK; r++) cpAsync4(&s.rank[r * kMergeCap + e], rk + r);
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < kItems; j++) {
+        const uint32_t e = threadIdx.x + j * kMergeThreads;
+        extra[j] = 0;
+        before[j] = 0;
+        if (e < size) {
+            const uint64_t bit = static_cast<uint64_t>(p[j]) * bits;
+            const uint64_t w0 = bit >> 6;
+            extra[j] = __ldg(a.texts.packed + w0 + W);
+            if ((bit & 63) < bits && w0 > 0) before[j] = __ldg(a.texts.packed + w0 - 1);
+        }
+    }
+    cpAsyncWaitAll();
+#pragma unroll
+    for (int j = 0; j < kItems; j++) {
+        const uint32_t e = threadIdx.x + j * kMergeThreads;
+        if (e < size) {
+            const uint32_t o = static_cast<uint32_t>((static_cast<uint64_t>(p[j]) * bits) & 63);
+            uint64_t r[W + 1];
+#pragma unroll
+            for (int w = 0; w < W; w++) r[w] = s.words[w * kMergeCap + e];
+            r[W] = extra[j];
+            // the character before p ends at bit o of word 0: bits [64 + o - b, 64 + o) of before:r[0]
+            const uint64_t window = o ? (before[j] << o) | (r[0] >> (64 - o)) : before[j];
+            s.prev[e] = static_cast<uint8_t>(window & ((1u << bits) - 1));
+            if (o) {
+#pragma unroll
+                for (int w = 0; w < W; w++) s.words[w * kMergeCap + e] = (r[w] << o) | (r[w + 1] >> (64 - o));
+            }
+        }
+    }
+    __syncthreads();
+
+    // The merge tree.
+    finalLevel(s, s.idxA, s.idxB, bounds, 4, size, n, bits, tb);
+    __syncthreads();
+    finalLevel(s, s.idxB, s.idxA, bounds + 12, 2, size, n, bits, tb);
+    __syncthreads();
+    finalLevel(s, s.idxA, s.idxB, bounds + 18, 1, size, n, bits, tb);
+    __syncthreads();
+    const uint16_t* order = s.idxB;
+
+    // Ranks of the tile's splitters in the window set bound the outputs this tile owns.
+    for (uint32_t r = threadIdx.x; r < size; r += kMergeThreads) {
+        const uint32_t x = order[r];
+        if (x == t.loIdx) sLo = r;
+        if (x == t.hiIdx) sHi = r;
+    }
+    __syncthreads();
+    const uint32_t lo = sLo, hi = sHi;
+    for (uint32_t r = lo + threadIdx.x; r < hi; r += kMergeThreads) {
+        const uint32_t x = order[r];
+        const uint32_t q = s.pos[x];
+        const uint32_t gIdx = t.base + r;
+        if (gIdx >= a.level.start[kClasses]) {  // cannot happen for a correct tiling; never write out of range
+            atomicExch(a.error, 2u);
+            continue;
+        }
+        const uint32_t tj = kMulti ? a.texts.textOf(q) : 0;
+        const uint32_t first = kMulti ? a.texts.startOf(tj) : 0;
+        if (a.sa) a.sa[gIdx] = q - first;
+        if (a.bwt && q != first) {
+            const uint32_t base = kMulti ? __ldg(a.outBase + tj) : 0;
+            const uint32_t row = gIdx - base, zero = __ldg(a.rowZero + tj);
+            a.bwt[base + (row < zero ? row + 1 : row)] = __ldg(a.texts.decode + s.prev[x]);
+        }
+    }
+}
+
+// Launches the final level for the texts' code width (W words per record) and text count.
+template <int W, bool kMulti>
+inline cudaError_t launchFinalFor(const MergeArgs& args, uint32_t tiles, cudaStream_t stream) {
+    constexpr size_t shared = FinalTile<W, kMulti>::sharedBytes();
+    static uint64_t configured = 0;
+    int device = 0;
+    SADCS_TRY(cudaGetDevice(&device));
+    if (!(configured >> (device & 63) & 1)) {
+        SADCS_TRY(cudaFuncSetAttribute(mergeFinal<W, kMulti>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(shared)));
+        configured |= uint64_t(1) << (device & 63);
+    }
+    return launch(mergeFinal<W, kMulti>, tiles, kMergeThreads, shared, stream, args);
+}
+
+template <bool kMulti>
+inline cudaError_t launchFinalMulti(const MergeArgs& args, uint32_t tiles, cudaStream_t stream) {
+    switch (finalWords(args.texts.bits)) {
+        case 1: return launchFinalFor<1, kMulti>(args, tiles, stream);
+        case 2: return launchFinalFor<2, kMulti>(args, tiles, stream);
+        case 3: return launchFinalFor<3, kMulti>(args, tiles, stream);
+        default: return launchFinalFor<4, kMulti>(args, tiles, stream);
+    }
+}
+
+inline cudaError_t launchFinal(const MergeArgs& args, uint32_t tiles, cudaStream_t stream) {
+    return args.texts.count > 1 ? launchFinalMulti<true>(args, tiles, stream)
+                                : launchFinalMulti<false>(args, tiles, stream);
+}
+
+}  // namespace sadcs

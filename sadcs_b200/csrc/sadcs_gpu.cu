@@ -25,6 +25,7 @@
 #include "classes.cuh"
 #include "common.cuh"
 #include "merge.cuh"
+#include "merge_final.cuh"
 #include "primitives.cuh"
 #include "rank.cuh"
 
