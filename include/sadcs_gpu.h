@@ -179,9 +179,9 @@ int sadcs_gpu_check_suffix_array(const uint8_t* d_text, int64_t n, const uint32_
  * with SADCS_FAILED and a message naming the limit; nothing is launched.
  * The first call on each device looks up the array's address (cudaGetSymbolAddress), which may load
  * the library's device code: make that first call before capturing any stream.
- * Initial values: each call sets its three result words itself (to all ones) before its kernels
- * run; the inverse-suffix-array words need none (every word the verdict depends on is written by
- * the same call).
+ * Initial values: the array keeps whatever the last call left; each call sets what must start
+ * known before its kernels run: its three result words to all ones and the first n words of the
+ * inverse suffix array to zero.
  * All calls on one device share that one array: calls that overlap in time (on other streams or
  * from other threads) race on it and their verdicts are undefined - serialise them. */
 #define SADCS_GPU_STATIC_CHECK_MAX 1048576

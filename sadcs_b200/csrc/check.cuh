@@ -20,6 +20,9 @@ namespace sadcs {
 
 constexpr uint64_t kNoFailure = ~uint64_t(0);
 
+// isa[p] = the largest i with sa[i] = p (isa zeroed by the caller), so that of equal entries the
+// last one owns the slot whatever the order of the writes, as in a sequential scatter: the first
+// duplicate reported is then the smallest index of any repeated entry, on every run.
 __global__ void checkScatter(const uint32_t* __restrict__ sa, uint32_t n, uint32_t* __restrict__ isa,
                              unsigned long long* __restrict__ firstBad) {
     const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -28,7 +31,7 @@ __global__ void checkScatter(const uint32_t* __restrict__ sa, uint32_t n, uint32
     if (p >= n) {
         atomicMin(firstBad, static_cast<unsigned long long>(i));
     } else {
-        isa[p] = static_cast<uint32_t>(i);
+        atomicMax(isa + p, static_cast<uint32_t>(i));
     }
 }
 

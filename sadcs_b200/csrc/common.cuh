@@ -71,6 +71,30 @@ constexpr Cover makeCover() {
 }
 
 constexpr Cover kCoverTables = makeCover();
+
+// The cover as a bit mask (bit r set for r in D) and its rotations: bit t of coverRotation(a) is
+// set when a + t is sampled. The tie offset of residues a, b is the lowest bit set in both
+// rotations, and the slot of sample a + k among the samples of [a, a + 32) is the number of bits
+// of coverRotation(a) below k: two register instructions each instead of table lookups.
+constexpr uint32_t coverMask() {
+    uint32_t m = 0;
+    for (int r = 0; r < kV; r++) m |= coverHas(r) ? (1u << r) : 0u;
+    return m;
+}
+constexpr uint32_t kCoverMask = coverMask();
+static_assert(kCoverMask == 0x0208110Bu, "cover mask");
+
+__device__ __forceinline__ uint32_t coverRotation(uint32_t p) {
+    return __funnelshift_r(kCoverMask, kCoverMask, p);  // rotate right by p mod 32
+}
+
+__device__ __forceinline__ uint32_t tieOffset(uint32_t rotA, uint32_t rotB) {
+    return static_cast<uint32_t>(__ffs(rotA & rotB)) - 1;
+}
+
+__device__ __forceinline__ uint32_t sampleSlot(uint32_t rotA, uint32_t k) {
+    return static_cast<uint32_t>(__popc(rotA & ((1u << k) - 1)));
+}
 static_assert(kCoverTables.classOf[2] == 1 && kCoverTables.classOf[26] == 6, "cover tables");
 
 __constant__ Cover cCover = makeCover();

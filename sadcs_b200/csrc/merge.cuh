@@ -30,7 +30,12 @@
 namespace sadcs {
 
 constexpr uint32_t kMergeG = 32;
-constexpr uint32_t kMergeR = 30;  // with G = 32: tiles of at most 1147 records
+// Rows every R splitters; tiles of at most G * R + 6 * (G - 1) + 1 records (1147 at R = 30). R sets the
+// tile's shared memory and so the blocks per SM; the build may override it (tuning).
+#ifndef SADCS_MERGE_R
+#define SADCS_MERGE_R 30
+#endif
+constexpr uint32_t kMergeR = SADCS_MERGE_R;
 constexpr uint32_t kMergeCap = kMergeG * kMergeR + 6 * (kMergeG - 1) + 1;
 constexpr int kMergeThreads = 256;
 constexpr int kPairs = kClasses * (kClasses - 1) / 2;

@@ -48,33 +48,60 @@ struct FinalTile {
     }
 };
 
-// Suffix x < suffix y (record indices of the tile), by the difference-cover comparison
-// (merge.cuh: lessRecord) on the shared-memory fields.
+// The fields of a record a comparison reads first, kept in registers while the merge walk holds
+// the record.
+struct FinalHead {
+    uint32_t idx, pos, rot, end;  // rot: coverRotation(pos); end: several texts only
+    uint64_t w0;
+};
+
 template <int W, bool kMulti>
-__device__ __forceinline__ bool finalLess(const FinalTile<W, kMulti>& s, uint32_t x, uint32_t y, uint32_t n,
-                                          uint32_t bits, const MergeTables& tb) {
+__device__ __forceinline__ FinalHead loadHead(const FinalTile<W, kMulti>& s, uint32_t x) {
+    FinalHead h;
+    h.idx = x;
+    h.pos = s.pos[x];
+    h.rot = coverRotation(h.pos);
+    h.w0 = s.words[x];
+    h.end = kMulti ? s.end[x] : 0;
+    return h;
+}
+
+// Suffix a < suffix b, by the difference-cover comparison (merge.cuh: lessRecord): texts by their
+// end, then the first k = tie offset characters (at most the shorter suffix's length), then the
+// sample ranks at a + k and b + k; a suffix that is a prefix of the other is the smaller.
+template <int W, bool kMulti>
+__device__ __forceinline__ bool headLess(const FinalTile<W, kMulti>& s, const FinalHead& a, const FinalHead& b,
+                                         uint32_t n, uint32_t bits) {
     if constexpr (kMulti) {
-        const uint32_t ex = s.end[x], ey = s.end[y];
-        if (ex != ey) return ex < ey;  // different texts: text order
-        n = ex;
+        if (a.end != b.end) return a.end < b.end;  // different texts: text order
+        n = a.end;
     }
-    const uint32_t i = s.pos[x], j = s.pos[y];
-    const uint32_t k = tb.tie[i % kV][j % kV];
+    const uint32_t i = a.pos, j = b.pos;
+    const uint32_t k = tieOffset(a.rot, b.rot);
     const uint32_t common = min(k, min(n - i, n - j));
     const uint32_t cbits = common * bits;
+    {
+        uint64_t x = a.w0, y = b.w0;
+        if (cbits < 64) {
+            const uint64_t mk = cbits ? ~uint64_t(0) << (64 - cbits) : 0;
+            x &= mk;
+            y &= mk;
+        }
+        if (x != y) return x < y;
+    }
 #pragma unroll
-    for (int w = 0; w < W; w++) {
+    for (int w = 1; w < W; w++) {
         if (cbits <= 64u * w) break;
-        uint64_t a = s.words[w * kMergeCap + x], b = s.words[w * kMergeCap + y];
+        uint64_t x = s.words[w * kMergeCap + a.idx], y = s.words[w * kMergeCap + b.idx];
         if (cbits < 64u * (w + 1)) {
             const uint64_t mk = ~uint64_t(0) << (64u * (w + 1) - cbits);
-            a &= mk;
-            b &= mk;
+            x &= mk;
+            y &= mk;
         }
-        if (a != b) return a < b;
+        if (x != y) return x < y;
     }
     if (common < k || i + k == n || j + k == n) return i > j;  // one is a prefix of the other
-    return s.rank[tb.slot[i % kV][k] * kMergeCap + x] < s.rank[tb.slot[j % kV][k] * kMergeCap + y];
+    return s.rank[sampleSlot(a.rot, k) * kMergeCap + a.idx] < s.rank[sampleSlot(b.rot, k) * kMergeCap + b.idx];
 }
 
 // One tree level: the merges m (A = [mb[3m], mb[3m + 1]), B = [mb[3m + 1], mb[3m + 2]) of src,
@@ -82,8 +109,8 @@ __device__ __forceinline__ bool finalLess(const FinalTile<W, kMulti>& s, uint32_
 // writes outputs [t * chunk, (t + 1) * chunk).
 template <int W, bool kMulti>
 __device__ __forceinline__ void finalLevel(const FinalTile<W, kMulti>& s, const uint16_t* src, uint16_t* dst,
-                                           const uint32_t* mb, int merges, uint32_t size, uint32_t n, uint32_t bits,
-                                           const MergeTables& tb) {
+                                           const uint32_t* mb, int merges, uint32_t size, uint32_t n,
+                                           uint32_t bits) {
     const uint32_t chunk = (size + kMergeThreads - 1) / kMergeThreads;
     uint32_t at = threadIdx.x * chunk;
     const uint32_t stopAll = min(at + chunk, size);
@@ -97,23 +124,25 @@ __device__ __forceinline__ void finalLevel(const FinalTile<W, kMulti>& s, const 
         uint32_t lo = d > lenB ? d - lenB : 0, hi = min(d, lenA);
         while (lo < hi) {
             const uint32_t mid = (lo + hi) >> 1;
-            if (finalLess(s, src[a0 + mid], src[a1 + d - 1 - mid], n, bits, tb)) {
+            if (headLess(s, loadHead(s, src[a0 + mid]), loadHead(s, src[a1 + d - 1 - mid]), n, bits)) {
                 lo = mid + 1;
             } else {
                 hi = mid;
             }
         }
         uint32_t i = lo, j = d - lo;
-        uint32_t xa = i < lenA ? src[a0 + i] : 0, xb = j < lenB ? src[a1 + j] : 0;
+        FinalHead ha{}, hb{};
+        if (i < lenA) ha = loadHead(s, src[a0 + i]);
+        if (j < lenB) hb = loadHead(s, src[a1 + j]);
         for (; d < stop; d++) {
-            if (j == lenB || (i < lenA && finalLess(s, xa, xb, n, bits, tb))) {
-                dst[a0 + d] = static_cast<uint16_t>(xa);
+            if (j == lenB || (i < lenA && headLess(s, ha, hb, n, bits))) {
+                dst[a0 + d] = static_cast<uint16_t>(ha.idx);
                 i++;
-                if (i < lenA) xa = src[a0 + i];
+                if (i < lenA) ha = loadHead(s, src[a0 + i]);
             } else {
-                dst[a0 + d] = static_cast<uint16_t>(xb);
+                dst[a0 + d] = static_cast<uint16_t>(hb.idx);
                 j++;
-                if (j < lenB) xb = src[a1 + j];
+                if (j < lenB) hb = loadHead(s, src[a1 + j]);
             }
         }
         at = a0 + stop;
@@ -126,17 +155,8 @@ __global__ void __launch_bounds__(kMergeThreads) mergeFinal(MergeArgs a) {
     FinalTile<W, kMulti> s;
     s.carve(smem);
     __shared__ MergeTileInfo t;
-    __shared__ __align__(16) MergeTables tb;
     __shared__ uint32_t sLo, sHi;
     __shared__ uint32_t bounds[3 * 7];  // the tree's merges: 4 + 2 + 1 triples of window offsets
-    {
-        const uint32_t* src = reinterpret_cast<const uint32_t*>(&cCover.tie[0][0]);
-        uint32_t* dst = reinterpret_cast<uint32_t*>(&tb.tie[0][0]);
-        for (int i = threadIdx.x; i < kV * kV / 4; i += kMergeThreads) dst[i] = src[i];
-        const uint32_t* src2 = reinterpret_cast<const uint32_t*>(&cCover.slot[0][0]);
-        uint32_t* dst2 = reinterpret_cast<uint32_t*>(&tb.slot[0][0]);
-        for (int i = threadIdx.x; i < kV * kV / 4; i += kMergeThreads) dst2[i] = src2[i];
-    }
     if (threadIdx.x == 0) {
         planTileWindows(a, t);
         sLo = 0;
@@ -217,11 +237,11 @@ __global__ void __launch_bounds__(kMergeThreads) mergeFinal(MergeArgs a) {
     __syncthreads();
 
     // The merge tree.
-    finalLevel(s, s.idxA, s.idxB, bounds, 4, size, n, bits, tb);
+    finalLevel(s, s.idxA, s.idxB, bounds, 4, size, n, bits);
     __syncthreads();
-    finalLevel(s, s.idxB, s.idxA, bounds + 12, 2, size, n, bits, tb);
+    finalLevel(s, s.idxB, s.idxA, bounds + 12, 2, size, n, bits);
     __syncthreads();
-    finalLevel(s, s.idxA, s.idxB, bounds + 18, 1, size, n, bits, tb);
+    finalLevel(s, s.idxA, s.idxB, bounds + 18, 1, size, n, bits);
     __syncthreads();
     const uint16_t* order = s.idxB;
 

@@ -921,6 +921,7 @@ int sadcs_gpu_check_suffix_array(const uint8_t* d_text, int64_t n, const uint32_
     }
     const uint32_t blocks = (count + 255) / 256;
     error = cudaMemsetAsync(words, 0xFF, 3 * sizeof(unsigned long long), st);
+    if (error == cudaSuccess) error = cudaMemsetAsync(isa, 0, 4 * static_cast<size_t>(count), st);
     if (error == cudaSuccess) error = launch(checkScatter, blocks, 256, 0, st, d_sa, count, isa, words);
     if (error == cudaSuccess) error = cudaMemcpyAsync(host, words, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
     if (error == cudaSuccess) error = cudaStreamSynchronize(st);
@@ -959,9 +960,9 @@ int sadcs_gpu_check_suffix_array(const uint8_t* d_text, int64_t n, const uint32_
 namespace {
 
 // Scratch of sadcs_gpu_check_suffix_array_static, in module memory: three 64-bit result words at
-// word 0 (set to all ones by every call), the inverse suffix array from word 64 (no initial value
-// needed: each word a verdict reads is written by the same call's scatter). Shared by every call on
-// a device, so overlapping calls race.
+// word 0 (set to all ones by every call), the inverse suffix array from word 64 (its first n words
+// set to zero by every call: the scatter keeps the largest index per entry). Shared by every call
+// on a device, so overlapping calls race.
 constexpr int64_t kStaticCheckMax = SADCS_GPU_STATIC_CHECK_MAX;
 constexpr size_t kStaticCheckIsaWord = 64;
 static __device__ __align__(256) uint32_t gStaticCheckScratch[kStaticCheckIsaWord + kStaticCheckMax];
@@ -1010,6 +1011,7 @@ int sadcs_gpu_check_suffix_array_static(const uint8_t* d_text, int64_t n, const 
     unsigned long long host[3] = {kNoFailure, kNoFailure, kNoFailure};  // pageable: nothing is allocated
     const uint32_t blocks = (count + 255) / 256;
     error = cudaMemsetAsync(words, 0xFF, 3 * sizeof(unsigned long long), st);
+    if (error == cudaSuccess) error = cudaMemsetAsync(isa, 0, 4 * static_cast<size_t>(count), st);
     if (error == cudaSuccess) error = launch(checkScatter, blocks, 256, 0, st, d_sa, count, isa, words);
     if (error == cudaSuccess) error = cudaMemcpyAsync(host, words, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
     if (error == cudaSuccess) error = cudaStreamSynchronize(st);
