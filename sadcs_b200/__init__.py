@@ -426,11 +426,18 @@ class Server:
         self._handle = handle
         self._pending = {}
 
-    def submit(self, text) -> int:
+    def submit(self, text, sa: np.ndarray | None = None, bwt: np.ndarray | None = None) -> int:
+        """Queues a text; sa (uint32, n) and bwt (uint8, n) may be given as the output buffers (for
+        instance page-locked ones, which the device copies into directly)."""
         t = _as_text(text)
         n = len(t)
-        sa = np.empty(max(n, 1), np.uint32)
-        out = np.empty(max(n, 1), np.uint8)
+        if sa is None:
+            sa = np.empty(max(n, 1), np.uint32)
+        if bwt is None:
+            bwt = np.empty(max(n, 1), np.uint8)
+        if sa.dtype != np.uint32 or bwt.dtype != np.uint8 or len(sa) < n or len(bwt) < n:
+            raise ValueError("sa must be uint32 and bwt uint8, each of at least n entries")
+        out = bwt
         ticket = ctypes.c_uint64(0)
         _check(lib().sadcs_gpu_server_submit(self._handle, t.ctypes.data_as(_u8p), n, sa.ctypes.data_as(_u32p),
                                              out.ctypes.data_as(_u8p), ctypes.byref(ticket)))

@@ -163,32 +163,76 @@ __global__ void __launch_bounds__(256) byteHistogram(const uint8_t* __restrict__
     if (h[threadIdx.x]) atomicAdd(counts + threadIdx.x, h[threadIdx.x]);
 }
 
+// The stable pass by byte runs over chunks of kInverseChunk positions, each a segment with its own
+// digit bases (the digit's start plus its count in the chunks before), so that no segment reaches the
+// 2^30 counts a look-back word holds; one chunk below that size.
+constexpr uint32_t kInverseChunk = 1u << 29;
+constexpr uint32_t kInverseMaxChunks = 8;  // n < 2^32
+
+// elementStart[s] / tileStart[s] of the chunks (s = 0..chunks). One thread per entry.
+__global__ void inverseChunkTables(uint32_t n, uint32_t chunks, uint32_t* __restrict__ elementStart,
+                                   uint32_t* __restrict__ tileStart) {
+    const uint32_t s = threadIdx.x;
+    if (s > chunks) return;
+    const uint64_t e = min(static_cast<uint64_t>(s) * kInverseChunk, static_cast<uint64_t>(n));
+    elementStart[s] = static_cast<uint32_t>(e);
+    tileStart[s] = static_cast<uint32_t>((e + kSortTile - 1) / kSortTile);
+}
+
+// hist[s][d] (byte counts of chunk s) becomes the first output slot of byte d in chunk s: every
+// smaller byte, then byte d in the chunks before. One block of 256 threads.
+__global__ void __launch_bounds__(256) inverseChunkBases(uint32_t* __restrict__ hist, uint32_t chunks) {
+    __shared__ uint32_t warpTotals[32];
+    const uint32_t d = threadIdx.x;
+    uint32_t total = 0;
+    for (uint32_t s = 0; s < chunks; s++) total += hist[s * 256 + d];
+    uint32_t all;
+    const uint32_t inclusive = blockInclusiveScan<OpSum>(total, warpTotals, all);
+    uint32_t base = inclusive - total;
+    for (uint32_t s = 0; s < chunks; s++) {
+        const uint32_t c = hist[s * 256 + d];
+        hist[s * 256 + d] = base;
+        base += c;
+    }
+}
+
 // Inverts bwt (n bytes, primary) into text (n bytes) on the device. scratch: inverseScratchWords(n)
 // words; hostWord: one page-locked word. *valid = false if the BWT is not a valid one (rows that
 // never reach the primary row).
 inline size_t inverseScratchWords(uint64_t n) {
-    return 6 * static_cast<size_t>(n + 1) + radixScratchWords(n) + 512 + 64;
+    return 6 * static_cast<size_t>(n + 1) + 512 + radixScratchWords(n) + kInverseMaxChunks * 256 + 64;
 }
 
 inline cudaError_t inverseBwt(const uint8_t* bwt, uint32_t n, uint32_t primary, uint8_t* text, uint32_t* scratch,
                               uint32_t* hostWord, cudaStream_t stream, bool& valid) {
     valid = true;
     if (n == 0) return cudaSuccess;
-    uint32_t* sorted = scratch;                   // n + 1
-    uint32_t* lf = sorted + (n + 1);              // n + 1
-    uint32_t* next[2] = {lf + (n + 1), lf + 2 * (n + 1)};
-    uint32_t* dist[2] = {next[1] + (n + 1), next[1] + 2 * (n + 1)};
-    uint32_t* words = dist[1] + (n + 1);          // [0..255] counts, [256] changed / bad
+    const size_t rows = static_cast<size_t>(n) + 1;  // offsets in 64 bits: 2 * rows passes 2^32 for n >= 2^31
+    uint32_t* sorted = scratch;                   // rows
+    uint32_t* lf = sorted + rows;                 // rows
+    uint32_t* next[2] = {lf + rows, lf + 2 * rows};
+    uint32_t* dist[2] = {next[1] + rows, next[1] + 2 * rows};
+    uint32_t* words = dist[1] + rows;             // [256] changed, [258..259] first bad row
     uint32_t* radixWords = words + 512;
+    uint32_t* hist = radixWords + radixScratchWords(n);  // [chunks][256], then the chunk tables
+    uint32_t* elementStart = hist + kInverseMaxChunks * 256;  // 16 words, then tileStart (16)
+    uint32_t* tileStart = elementStart + 16;
+    const uint32_t chunks = ceilDiv(n, kInverseChunk);
     const RadixScratch radix(radixWords, n);
     SADCS_TRY(cudaMemsetAsync(words, 0, 512 * 4, stream));
     SADCS_TRY(cudaMemsetAsync(radix.control, 0, 8, stream));
-    const uint32_t histBlocks = std::min<uint32_t>(ceilDiv(n, 256 * 16), 148 * 8);
-    SADCS_TRY(launch(byteHistogram, histBlocks, 256, 0, stream, bwt, n, words));
-    SADCS_TRY(launch(radixDigitBase, 1, 256, 0, stream, words));
-    SADCS_TRY((radixOnesweepPass<uint8_t, ByteLoader, ValueStorer>(ByteLoader{bwt}, ValueStorer{sorted, n},
-                                                                    OneSegment{n}, n, ceilDiv(n, kSortTile), words,
-                                                                    radix, stream)));
+    SADCS_TRY(cudaMemsetAsync(hist, 0, static_cast<size_t>(chunks) * 256 * 4, stream));
+    for (uint32_t c = 0; c < chunks; c++) {
+        const uint32_t count = std::min<uint32_t>(kInverseChunk, n - c * kInverseChunk);
+        const uint32_t histBlocks = std::min<uint32_t>(ceilDiv(count, 256 * 16), 148 * 8);
+        SADCS_TRY(launch(byteHistogram, histBlocks, 256, 0, stream, bwt + static_cast<size_t>(c) * kInverseChunk,
+                         count, hist + static_cast<size_t>(c) * 256));
+    }
+    SADCS_TRY(launch(inverseChunkBases, 1, 256, 0, stream, hist, chunks));
+    SADCS_TRY(launch(inverseChunkTables, 1, 32, 0, stream, n, chunks, elementStart, tileStart));
+    SADCS_TRY((radixOnesweepPass<uint8_t, ByteLoader, ValueStorer, ManySegments>(
+        ByteLoader{bwt}, ValueStorer{sorted, n}, ManySegments{tileStart, elementStart, chunks}, n, ceilDiv(n, kSortTile),
+        hist, radix, stream)));
     SADCS_TRY(launch(lfScatter, ceilDiv(n, 256), 256, 0, stream, sorted, n, lf));
     SADCS_TRY(launch(lfInitRows, ceilDiv(n + 1ull, 256), 256, 0, stream, lf, n, primary, next[0], dist[0]));
     int cur = 0;

@@ -21,6 +21,14 @@
 
 namespace sadcs {
 
+// Shared-memory share of the unified L1/shared array preferred for the final level, in percent of
+// the maximum (-1: the driver's choice). The record gathers go through L1 and the kernel runs 40%
+// slower with 28 KB of L1 than with 60 KB: 85% gives 196 KB of shared memory (3 tiles of natural
+// text per SM) and 60 KB of L1; the driver's own choice would take all 228 KB when the tiles fit.
+#ifndef SADCS_MERGE_CARVEOUT
+#define SADCS_MERGE_CARVEOUT 85
+#endif
+
 // 64-bit words of the code stream a final-level record keeps: 31 characters of `bits` bits.
 __host__ __device__ constexpr int finalWords(uint32_t bits) {
     return static_cast<int>((31 * bits + 63) / 64);
@@ -282,6 +290,10 @@ inline cudaError_t launchFinalFor(const MergeArgs& args, uint32_t tiles, cudaStr
     if (!(configured >> (device & 63) & 1)) {
         SADCS_TRY(cudaFuncSetAttribute(mergeFinal<W, kMulti>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(shared)));
+#if SADCS_MERGE_CARVEOUT >= 0
+        SADCS_TRY(cudaFuncSetAttribute(mergeFinal<W, kMulti>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                       SADCS_MERGE_CARVEOUT));
+#endif
         configured |= uint64_t(1) << (device & 63);
     }
     return launch(mergeFinal<W, kMulti>, tiles, kMergeThreads, shared, stream, args);

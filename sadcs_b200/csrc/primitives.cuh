@@ -14,6 +14,7 @@
 #pragma once
 
 #include <algorithm>
+#include <type_traits>
 
 #include "common.cuh"
 
@@ -164,8 +165,8 @@ cudaError_t deviceScan(const uint32_t* in, uint32_t* out, uint32_t count, uint32
 // counts, and looks back over the tiles before it for their running totals (decoupled look-back).
 // The global digit offsets come from one histogram pass made beforehand (for all digits of a sort
 // at once). Tiles are numbered in the order blocks start, so a tile's predecessors are resident or
-// done and the look-back ends; it is still bounded by %globaltimer: past the limit a block sets
-// the error word and stores nothing. Counts stay below 2^30 (flags in the top 2 bits).
+// done and the look-back ends; it is still bounded by the SM cycle counter: past the limit a block
+// sets the error word and stores nothing. Counts stay below 2^30 (flags in the top 2 bits).
 
 constexpr int kSortThreads = 256;
 constexpr int kSortWarps = kSortThreads / 32;
@@ -176,13 +177,10 @@ constexpr uint32_t kStatusAggregate = 1u << 30;
 constexpr uint32_t kStatusPrefix = 2u << 30;
 constexpr uint32_t kStatusValue = (1u << 30) - 1;
 constexpr uint32_t kMaxSortCount = kStatusValue;
-constexpr uint64_t kLookbackLimitNs = 2000000000ull;  // 2 s: far above any real wait
-
-__device__ __forceinline__ uint64_t globalTimerNs() {
-    uint64_t t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
+// The look-back gives up after this many SM cycles of waiting (2 s at the B200's 1965 MHz, longer at
+// lower clocks): far above any real wait. The SM's own cycle counter is monotonic for the thread
+// that reads it; a global-timer reading can jump when its two halves are read across a carry.
+constexpr long long kLookbackLimitCycles = 4000000000ll;
 
 // Shared memory of radixOnesweep for a staged key of keyBytes bytes.
 constexpr size_t radixSharedBytes(size_t keyBytes) {
@@ -295,15 +293,15 @@ __global__ void __launch_bounds__(kSortThreads, 2) radixOnesweep(Loader ld, Stor
     } else {
         vs[static_cast<size_t>(tile) * 256 + d] = kStatusAggregate | digitTotal;
         uint32_t t = tile;
-        uint64_t waitStart = 0;
+        long long waitStart = -1;
         bool failed = false;
         while (t > firstTile) {
             const uint32_t s = vs[static_cast<size_t>(t - 1) * 256 + d];
             if ((s & ~kStatusValue) == 0) {
-                const uint64_t now = globalTimerNs();
-                if (waitStart == 0) {
+                const long long now = clock64();
+                if (waitStart < 0 || now < waitStart) {
                     waitStart = now;
-                } else if (now - waitStart > kLookbackLimitNs) {
+                } else if (now - waitStart > kLookbackLimitCycles) {
                     failed = true;
                     break;
                 }
@@ -452,7 +450,9 @@ cudaError_t radixOnesweepPass(const Loader& ld, const Storer& st, const Segments
                               uint32_t tiles, const uint32_t* digitBase, const RadixScratch& scratch,
                               cudaStream_t stream) {
     if (count == 0 || tiles == 0) return cudaSuccess;
-    if (count > kMaxSortCount) return cudaErrorInvalidValue;
+    // A look-back word holds counts below 2^30: one segment at most that long (callers of the
+    // segmented passes keep every segment below it).
+    if (std::is_same<Segments, OneSegment>::value && count > kMaxSortCount) return cudaErrorInvalidValue;
     // status words and the tile counter start at zero; the error word is kept.
     SADCS_TRY(cudaMemsetAsync(scratch.status, 0, static_cast<size_t>(tiles) * 256 * 4, stream));
     SADCS_TRY(cudaMemsetAsync(scratch.control, 0, 4, stream));

@@ -392,7 +392,8 @@ cudaError_t prepareAlphabet(const uint8_t* text, uint64_t total, uint64_t span, 
 // Where a construction's inputs come from and its outputs go.
 struct Io {
     const uint8_t* hostText = nullptr;    // packed host texts, or
-    const uint8_t* deviceText = nullptr;  // packed device texts
+    const uint8_t* deviceText = nullptr;  // packed device texts, or
+    const uint8_t* const* hostPieces = nullptr;  // one host buffer per text (a batch of several)
     bool wantSa = false, wantBwt = false;
     uint32_t* outSa = nullptr;            // device outputs (caller-owned), or null for the slab's
     uint8_t* outBwt = nullptr;
@@ -466,10 +467,19 @@ int construct(sadcs_gpu_context* c, const Batch& b, Io& io, cudaStream_t stream,
     } else {
         uint8_t* staging = slab + L.staging;
         uint32_t* packedOffset = reinterpret_cast<uint32_t*>(slab + L.packed);  // free until the codes are packed
-        if ((error = cudaMemcpyAsync(staging, source, b.outputs,
-                                     io.hostText ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, stream)) !=
-                cudaSuccess ||
-            (error = cudaMemcpyAsync(packedOffset, dOutBase, 4 * static_cast<size_t>(J), cudaMemcpyDeviceToDevice,
+        if (io.hostPieces) {
+            for (uint32_t j = 0; j < J; j++) {
+                if ((error = cudaMemcpyAsync(staging + b.outBase[j], io.hostPieces[j], b.lengths[j],
+                                             cudaMemcpyHostToDevice, stream)) != cudaSuccess) {
+                    return failed("upload", error);
+                }
+            }
+        } else if ((error = cudaMemcpyAsync(staging, source, b.outputs,
+                                            io.hostText ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice,
+                                            stream)) != cudaSuccess) {
+            return failed("upload", error);
+        }
+        if ((error = cudaMemcpyAsync(packedOffset, dOutBase, 4 * static_cast<size_t>(J), cudaMemcpyDeviceToDevice,
                                      stream)) != cudaSuccess) {
             return failed("upload", error);
         }
@@ -480,8 +490,8 @@ int construct(sadcs_gpu_context* c, const Batch& b, Io& io, cudaStream_t stream,
             return failed("placing the texts", error);
         }
     }
-    if (io.hostText) {
-        s.pinned = isPinned(io.hostText) ? 1 : 0;
+    if (io.hostText || io.hostPieces) {
+        s.pinned = isPinned(io.hostText ? io.hostText : io.hostPieces[0]) ? 1 : 0;
         if ((error = cudaStreamSynchronize(stream)) != cudaSuccess) return failed("upload", error);
         s.upload_seconds = secondsSince(start);
     }

@@ -65,8 +65,8 @@ size_t footprintOf(const Batch& b) {
     return planLayout(extentOf(b), true, true).peak;
 }
 
-void serveBatch(sadcs_gpu_server* srv, sadcs_gpu_context& ctx, std::vector<ServerRequest*>& group, uint8_t* staging,
-                size_t stagingBytes, const Batch& b, size_t footprint) {
+void serveBatch(sadcs_gpu_server* srv, sadcs_gpu_context& ctx, std::vector<ServerRequest*>& group, const Batch& b,
+                size_t footprint) {
     sadcs_gpu_stats stats{};
     int status = SADCS_OK;
     std::string message;
@@ -85,16 +85,14 @@ void serveBatch(sadcs_gpu_server* srv, sadcs_gpu_context& ctx, std::vector<Serve
         Io io;
         io.wantSa = true;
         io.wantBwt = true;
+        std::vector<const uint8_t*> pieces;
         if (group.size() == 1) {
             io.hostText = group[0]->text;
         } else {
-            size_t at = 0;
-            for (ServerRequest* r : group) {
-                if (at + r->n > stagingBytes) break;
-                memcpy(staging + at, r->text, r->n);
-                at += r->n;
-            }
-            io.hostText = staging;
+            // Each request's text goes straight from the caller's buffer into the device staging
+            // region (asynchronous from page-locked memory; the driver stages pageable memory).
+            for (ServerRequest* r : group) pieces.push_back(r->text);
+            io.hostPieces = pieces.data();
         }
         status = construct(&ctx, b, io, ctx.stream, stats);
         if (status == SADCS_OK) {
@@ -141,10 +139,8 @@ void serverWorker(sadcs_gpu_server* srv) {
     sadcs_gpu_context ctx;
     ctx.device = srv->device;
     ctx.hostWordCount = 64 + metaWords(srv->batchTexts, 0) + 2 * static_cast<size_t>(srv->batchTexts) + 64 + 256;
-    uint8_t* staging = nullptr;
     bool ready = cudaStreamCreateWithFlags(&ctx.stream, cudaStreamNonBlocking) == cudaSuccess &&
-                 cudaMallocHost(&ctx.hostWords, 4 * ctx.hostWordCount) == cudaSuccess &&
-                 cudaMallocHost(&staging, std::max<size_t>(srv->batchBytes, 1)) == cudaSuccess;
+                 cudaMallocHost(&ctx.hostWords, 4 * ctx.hostWordCount) == cudaSuccess;
     for (cudaEvent_t& e : ctx.events) ready = ready && cudaEventCreate(&e) == cudaSuccess;
     for (;;) {
         std::vector<ServerRequest*> group;
@@ -203,14 +199,13 @@ void serverWorker(sadcs_gpu_server* srv) {
             srv->finished.notify_all();
             continue;
         }
-        serveBatch(srv, ctx, group, staging, srv->batchBytes, b, footprint);
+        serveBatch(srv, ctx, group, b, footprint);
     }
     for (cudaEvent_t& e : ctx.events) {
         if (e) cudaEventDestroy(e);
     }
     if (ctx.stream) cudaStreamDestroy(ctx.stream);
     if (ctx.hostWords) cudaFreeHost(ctx.hostWords);
-    if (staging) cudaFreeHost(staging);
     ctx.hostWords = nullptr;
     ctx.stream = nullptr;
 }

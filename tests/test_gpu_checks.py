@@ -63,3 +63,35 @@ def test_bwt_check_and_inverse():
                        ("primary 0", bwt, 0)):
         ok, _ = sa.check_bwt_device(d_text.data_ptr(), len(text), _device(b).data_ptr(), p)
         assert not ok, name
+
+
+def test_inverse_bwt_across_chunks_past_2g():
+    """Past 2^29 positions the inverse's stable byte pass runs as chunks with carried digit bases,
+    and past 2^31 its scratch offsets pass 2^32 words: a 2 GiB + 4 KiB text over {A,C,G,T} (five
+    chunks) built by this library must come back exactly, and one changed byte must be caught."""
+    import torch
+
+    n = (1 << 31) + 4099
+    g = torch.Generator(device="cuda").manual_seed(21)
+    d_text = torch.randint(0, 4, (n,), dtype=torch.uint8, device="cuda", generator=g)
+    d_text.mul_(2).add_(65)  # A C E G: four symbols, code order = byte order
+    d_sa = torch.empty(n, dtype=torch.int32, device="cuda")
+    d_bwt = torch.empty(n, dtype=torch.uint8, device="cuda")
+    ctx = sa.Context(n)
+    primary = sa.build_device(d_text.data_ptr(), n, d_sa.data_ptr(), d_bwt.data_ptr(), context=ctx)
+    ctx.close()
+    ok, where, _ = sa.check_suffix_array_device(d_text.data_ptr(), n, d_sa.data_ptr())
+    assert ok, where
+    del d_sa
+    torch.cuda.empty_cache()
+    out = torch.zeros(n, dtype=torch.uint8, device="cuda")
+    sa.inverse_bwt_device(d_bwt.data_ptr(), n, primary, out.data_ptr())
+    torch.cuda.synchronize()
+    assert torch.equal(out, d_text)
+    del out
+    torch.cuda.empty_cache()
+    ok, where = sa.check_bwt_device(d_text.data_ptr(), n, d_bwt.data_ptr(), primary)
+    assert ok, where
+    d_bwt[n - 7] ^= 2  # one changed byte in the last chunk
+    ok, _ = sa.check_bwt_device(d_text.data_ptr(), n, d_bwt.data_ptr(), primary)
+    assert not ok
