@@ -305,6 +305,7 @@ __global__ void __launch_bounds__(kSortThreads, 2) radixOnesweep(Loader ld, Stor
                     failed = true;
                     break;
                 }
+                __nanosleep(64);  // back off: spinning threads take issue slots and L2 bandwidth from other work
                 continue;
             }
             exclusive += s & kStatusValue;
