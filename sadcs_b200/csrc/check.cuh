@@ -129,18 +129,20 @@ __global__ void lfCompare(const uint8_t* __restrict__ a, const uint8_t* __restri
 
 struct ByteLoader {
     const uint8_t* __restrict__ bytes;
-    __device__ __forceinline__ bool load(uint32_t, uint32_t i, uint32_t, uint8_t& k, uint32_t& v, uint32_t& d) const {
+    __device__ __forceinline__ bool load(uint32_t, uint32_t i, uint32_t, uint8_t& k, uint32_t& d) const {
         k = bytes[i];
-        v = i;
         d = k;
         return true;
     }
+    __device__ __forceinline__ uint32_t value(uint32_t, uint32_t i, uint32_t) const { return i; }
 };
 
 struct ValueStorer {
+    static constexpr bool kKeys = false;
     uint32_t* __restrict__ out;
     uint32_t limit;
-    __device__ __forceinline__ void store(uint32_t, uint32_t pos, uint8_t, uint32_t v) const {
+    __device__ __forceinline__ void storeKey(uint32_t, uint32_t, uint8_t) const {}
+    __device__ __forceinline__ void storeValue(uint32_t, uint32_t pos, uint32_t v) const {
         if (pos < limit) out[pos] = v;
     }
 };

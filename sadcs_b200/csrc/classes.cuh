@@ -112,22 +112,26 @@ struct ClassLoader {
     const uint8_t* __restrict__ text;
     TextSet texts;
     uint32_t d;
-    __device__ __forceinline__ bool load(uint32_t j, uint32_t, uint32_t k, uint8_t& key, uint32_t& v,
-                                         uint32_t& dig) const {
+    __device__ __forceinline__ uint32_t element(uint32_t j, uint32_t k) const {
+        return k == 0 ? texts.endOfText(j) : lists[__ldg(prevOffset + j) + k - 1];
+    }
+    __device__ __forceinline__ bool load(uint32_t j, uint32_t, uint32_t k, uint8_t& key, uint32_t& dig) const {
         const uint32_t start = texts.startOf(j), end = texts.endOfText(j);
-        const uint32_t p = k == 0 ? end : lists[__ldg(prevOffset + j) + k - 1];
+        const uint32_t p = element(j, k);
         if (p <= start || p > end || cCover.classOf[(p - 1) % kV] != d) return false;
-        v = p - 1;
-        dig = charCode(texts, v);  // codes order like the bytes they stand for
+        dig = charCode(texts, p - 1);  // codes order like the bytes they stand for
         key = static_cast<uint8_t>(dig);
         return true;
     }
+    __device__ __forceinline__ uint32_t value(uint32_t j, uint32_t, uint32_t k) const { return element(j, k) - 1; }
 };
 
 struct ClassStorer {
+    static constexpr bool kKeys = false;
     uint32_t* __restrict__ lists;
     uint32_t lo, hi;  // class d's slots in the global lists
-    __device__ __forceinline__ void store(uint32_t, uint32_t pos, uint8_t, uint32_t v) const {
+    __device__ __forceinline__ void storeKey(uint32_t, uint32_t, uint8_t) const {}
+    __device__ __forceinline__ void storeValue(uint32_t, uint32_t pos, uint32_t v) const {
         if (pos >= lo && pos < hi) lists[pos] = v;  // always, unless a look-back timed out
     }
 };

@@ -182,9 +182,10 @@ constexpr uint32_t kMaxSortCount = kStatusValue;
 // that reads it; a global-timer reading can jump when its two halves are read across a carry.
 constexpr long long kLookbackLimitCycles = 4000000000ll;
 
-// Shared memory of radixOnesweep for a staged key of keyBytes bytes.
+// Shared memory of radixOnesweep for a key of keyBytes bytes: one staging buffer that holds the
+// tile's keys and then its values, the digit of every staged slot, and the counting tables.
 constexpr size_t radixSharedBytes(size_t keyBytes) {
-    return kSortTile * keyBytes + kSortTile * 4 + kSortTile + (kSortWarps * 256 + 256 + 256 + 32) * 4 + 64;
+    return kSortTile * (keyBytes > 4 ? keyBytes : 4) + kSortTile + (kSortWarps * 256 + 256 + 256 + 32) * 4 + 64;
 }
 
 // Segments of a pass: element ranges sorted independently, each from its own digit bases, with
@@ -220,16 +221,21 @@ struct ManySegments {
     }
 };
 
+// Loaders give, for (segment, element index in the pass, index within the segment), whether the
+// element takes part, its key and digit (load), and later its value (value, called again for the
+// same elements only, so that values are not held in registers through ranking and look-back).
+// Storers write keys (when kKeys) and values at output positions.
 template <class Key, class Loader, class Storer, class Segments = OneSegment>
-__global__ void __launch_bounds__(kSortThreads, 2) radixOnesweep(Loader ld, Storer st, Segments segs,
+__global__ void __launch_bounds__(kSortThreads, 3) radixOnesweep(Loader ld, Storer st, Segments segs,
                                                                  const uint32_t* __restrict__ digitBase,
                                                                  uint32_t* __restrict__ status,
                                                                  uint32_t* __restrict__ tileCounter,
                                                                  uint32_t* __restrict__ error) {
     extern __shared__ __align__(16) unsigned char smem[];
+    constexpr size_t kStageBytes = kSortTile * (sizeof(Key) > 4 ? sizeof(Key) : 4);
     Key* sKeys = reinterpret_cast<Key*>(smem);
-    uint32_t* sVals = reinterpret_cast<uint32_t*>(sKeys + kSortTile);
-    uint8_t* sDig = reinterpret_cast<uint8_t*>(sVals + kSortTile);
+    uint32_t* sVals = reinterpret_cast<uint32_t*>(smem);  // the same buffer, after the keys are out
+    uint8_t* sDig = smem + kStageBytes;
     uint32_t* warpCount = reinterpret_cast<uint32_t*>(sDig + kSortTile);
     uint32_t* digitStart = warpCount + kSortWarps * 256;
     uint32_t* digitGlobal = digitStart + 256;
@@ -254,15 +260,13 @@ __global__ void __launch_bounds__(kSortThreads, 2) radixOnesweep(Loader ld, Stor
     uint32_t* myCount = warpCount + warp * 256;
     const uint32_t lt = (1u << lane) - 1;
     Key keys[kSortItems];
-    uint32_t vals[kSortItems];
     uint32_t rankDigit[kSortItems];  // (rank within warp << 9) | digit
 
 #pragma unroll
     for (int j = 0; j < kSortItems; j++) {
         const uint64_t i = warpBase + j * 32 + lane;
         uint32_t d = kNoDigit;
-        if (!(i < count && ld.load(segment, segBegin + static_cast<uint32_t>(i), static_cast<uint32_t>(i), keys[j],
-                                   vals[j], d))) {
+        if (!(i < count && ld.load(segment, segBegin + static_cast<uint32_t>(i), static_cast<uint32_t>(i), keys[j], d))) {
             d = kNoDigit;
         }
         const uint32_t peers = __match_any_sync(0xffffffffu, d);
@@ -285,7 +289,8 @@ __global__ void __launch_bounds__(kSortThreads, 2) radixOnesweep(Loader ld, Stor
         digitTotal += c;
     }
 
-    // Publish, then look back for the running total of every earlier tile.
+    // Publish, then look back for the running total of every earlier tile, four tiles per step
+    // (independent loads), backing off while a predecessor has not published.
     volatile uint32_t* vs = status;
     uint32_t exclusive = 0;
     if (tile == firstTile) {
@@ -296,8 +301,27 @@ __global__ void __launch_bounds__(kSortThreads, 2) radixOnesweep(Loader ld, Stor
         long long waitStart = -1;
         bool failed = false;
         while (t > firstTile) {
-            const uint32_t s = vs[static_cast<size_t>(t - 1) * 256 + d];
-            if ((s & ~kStatusValue) == 0) {
+            constexpr uint32_t kWindow = 4;
+            const uint32_t avail = min(kWindow, t - firstTile);
+            uint32_t w[kWindow];
+#pragma unroll
+            for (uint32_t k = 0; k < kWindow; k++) w[k] = k < avail ? vs[static_cast<size_t>(t - 1 - k) * 256 + d] : 0;
+            uint32_t used = 0;
+            bool prefix = false, blocked = false;
+#pragma unroll
+            for (uint32_t k = 0; k < kWindow; k++) {
+                if (k >= avail || prefix || blocked) continue;
+                if ((w[k] & ~kStatusValue) == 0) {
+                    blocked = true;  // not published yet: resume from this tile
+                    continue;
+                }
+                exclusive += w[k] & kStatusValue;
+                used++;
+                if (w[k] & kStatusPrefix) prefix = true;
+            }
+            if (prefix) break;
+            t -= used;
+            if (blocked) {
                 const long long now = clock64();
                 if (waitStart < 0 || now < waitStart) {
                     waitStart = now;
@@ -306,11 +330,7 @@ __global__ void __launch_bounds__(kSortThreads, 2) radixOnesweep(Loader ld, Stor
                     break;
                 }
                 __nanosleep(64);  // back off: spinning threads take issue slots and L2 bandwidth from other work
-                continue;
             }
-            exclusive += s & kStatusValue;
-            t--;
-            if (s & kStatusPrefix) break;
         }
         if (failed) {
             sFailed = 1;
@@ -328,43 +348,81 @@ __global__ void __launch_bounds__(kSortThreads, 2) radixOnesweep(Loader ld, Stor
         return;
     }
 
+    // Staged slot of item j: its digit's start in the tile, the warps before, its rank in the warp.
+    uint32_t slot[kSortItems];
 #pragma unroll
     for (int j = 0; j < kSortItems; j++) {
         const uint32_t dj = rankDigit[j] & 0x1FF;
-        if (dj != kNoDigit) {
-            const uint32_t pos = digitStart[dj] + warpCount[warp * 256 + dj] + (rankDigit[j] >> 9);
-            sKeys[pos] = keys[j];
-            sVals[pos] = vals[j];
-            sDig[pos] = static_cast<uint8_t>(dj);
+        slot[j] = dj != kNoDigit ? digitStart[dj] + warpCount[warp * 256 + dj] + (rankDigit[j] >> 9) : 0xFFFFFFFFu;
+    }
+    if constexpr (Storer::kKeys) {
+#pragma unroll
+        for (int j = 0; j < kSortItems; j++) {
+            if (slot[j] != 0xFFFFFFFFu) {
+                sKeys[slot[j]] = keys[j];
+                sDig[slot[j]] = static_cast<uint8_t>(rankDigit[j] & 0xFF);
+            }
+        }
+        __syncthreads();
+        for (uint32_t i = threadIdx.x; i < tileTotal; i += kSortThreads) {
+            const uint32_t dj = sDig[i];
+            st.storeKey(segment, digitGlobal[dj] + i - digitStart[dj], sKeys[i]);
+        }
+        __syncthreads();
+    }
+    // Values, derived again by the loader for the same elements, staged in the same buffer.
+#pragma unroll
+    for (int j = 0; j < kSortItems; j++) {
+        if (slot[j] != 0xFFFFFFFFu) {
+            const uint64_t i = warpBase + j * 32 + lane;
+            sVals[slot[j]] = ld.value(segment, segBegin + static_cast<uint32_t>(i), static_cast<uint32_t>(i));
+            if constexpr (!Storer::kKeys) sDig[slot[j]] = static_cast<uint8_t>(rankDigit[j] & 0xFF);
         }
     }
     __syncthreads();
-
     for (uint32_t i = threadIdx.x; i < tileTotal; i += kSortThreads) {
         const uint32_t dj = sDig[i];
-        st.store(segment, digitGlobal[dj] + i - digitStart[dj], sKeys[i], sVals[i]);
+        st.storeValue(segment, digitGlobal[dj] + i - digitStart[dj], sVals[i]);
     }
 }
 
 // Digit histograms of a sort, all passes at once: hist[p * 256 + digit] (zeroed by the caller).
+// Each thread counts runs of equal digits in registers (one run per digit position) and adds a run
+// to the block's shared histogram only when its digit changes: a digit that is constant or nearly
+// so (the length tag of the ranking keys, the top byte of a skewed alphabet) costs almost no atomics,
+// and a random one one uncontended atomic per key. Warp-uniform trip counts are not needed (no
+// warp-synchronous instruction).
 template <class Key>
 __global__ void __launch_bounds__(256) radixHistogram(const Key* __restrict__ keys, uint32_t count, int beginBit,
                                                       int passes, uint32_t* __restrict__ hist) {
     __shared__ uint32_t h[8][256];
     for (int i = threadIdx.x; i < 8 * 256; i += blockDim.x) (&h[0][0])[i] = 0;
     __syncthreads();
-    const uint32_t lane = threadIdx.x & 31;
-    const uint32_t lt = (1u << lane) - 1;
+    uint32_t run[8], digit[8];
+#pragma unroll
+    for (int p = 0; p < 8; p++) {
+        run[p] = 0;
+        digit[p] = 0;
+    }
     const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
-    for (uint64_t base = static_cast<uint64_t>(blockIdx.x) * blockDim.x; base < count; base += stride) {
-        const uint64_t i = base + threadIdx.x;
-        const bool valid = i < count;
-        const Key k = valid ? keys[i] : Key(0);
-        for (int p = 0; p < passes; p++) {
-            const uint32_t dg = valid ? static_cast<uint32_t>(k >> (beginBit + 8 * p)) & 0xFF : kNoDigit;
-            const uint32_t peers = __match_any_sync(0xffffffffu, dg);
-            if (dg != kNoDigit && (peers & lt) == 0) atomicAdd(&h[p][dg], static_cast<uint32_t>(__popc(peers)));
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < count; i += stride) {
+        const Key k = keys[i];
+#pragma unroll
+        for (int p = 0; p < 8; p++) {
+            if (p < passes) {
+                const uint32_t dg = static_cast<uint32_t>(k >> (beginBit + 8 * p)) & 0xFF;
+                if (dg != digit[p]) {
+                    if (run[p]) atomicAdd(&h[p][digit[p]], run[p]);
+                    digit[p] = dg;
+                    run[p] = 0;
+                }
+                run[p]++;
+            }
         }
+    }
+#pragma unroll
+    for (int p = 0; p < 8; p++) {
+        if (p < passes && run[p]) atomicAdd(&h[p][digit[p]], run[p]);
     }
     __syncthreads();
     for (int i = threadIdx.x; i < passes * 256; i += blockDim.x) {
@@ -391,24 +449,25 @@ struct SortLoader {
     const Key* __restrict__ keys;
     const uint32_t* __restrict__ vals;
     int shift;
-    __device__ __forceinline__ bool load(uint32_t, uint32_t i, uint32_t, Key& k, uint32_t& v, uint32_t& d) const {
+    __device__ __forceinline__ bool load(uint32_t, uint32_t i, uint32_t, Key& k, uint32_t& d) const {
         k = keys[i];
-        v = vals[i];
         d = static_cast<uint32_t>(k >> shift) & 0xFF;
         return true;
     }
+    __device__ __forceinline__ uint32_t value(uint32_t, uint32_t i, uint32_t) const { return vals[i]; }
 };
 
 template <class Key>
 struct SortStorer {
+    static constexpr bool kKeys = true;
     Key* __restrict__ keys;
     uint32_t* __restrict__ vals;
     uint32_t limit;
-    __device__ __forceinline__ void store(uint32_t, uint32_t pos, Key k, uint32_t v) const {
-        if (pos < limit) {  // always, unless an earlier pass's look-back timed out
-            keys[pos] = k;
-            vals[pos] = v;
-        }
+    __device__ __forceinline__ void storeKey(uint32_t, uint32_t pos, Key k) const {
+        if (pos < limit) keys[pos] = k;  // always, unless an earlier pass's look-back timed out
+    }
+    __device__ __forceinline__ void storeValue(uint32_t, uint32_t pos, uint32_t v) const {
+        if (pos < limit) vals[pos] = v;
     }
 };
 

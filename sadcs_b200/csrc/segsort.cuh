@@ -91,7 +91,9 @@ __global__ void segCollectBig(const uint32_t* __restrict__ heads, uint32_t segme
     if (k == 0) tileStart[bigCount] = totalTiles;
 }
 
-// hist[(p * big + s) * 256 + digit] for every pass p of big segment s (zeroed by the caller).
+// hist[(p * big + s) * 256 + digit] for every pass p of big segment s (zeroed by the caller). Runs
+// of equal digits are counted in registers and added to the shared histogram when the digit
+// changes, as in radixHistogram.
 __global__ void __launch_bounds__(256) segHistogram(const uint64_t* __restrict__ keys, ListSegments segs,
                                                     uint32_t big, int passes, uint32_t* __restrict__ hist) {
     __shared__ uint32_t h[8][256];
@@ -100,17 +102,31 @@ __global__ void __launch_bounds__(256) segHistogram(const uint64_t* __restrict__
     uint32_t segment, firstTile, begin, size;
     segs.locate(blockIdx.x, segment, firstTile, begin, size);
     const uint32_t local = blockIdx.x - firstTile;
-    const uint32_t lt = (1u << (threadIdx.x & 31)) - 1;
     const uint32_t tileEnd = min((local + 1) * kSortTile, size);
-    for (uint32_t k0 = local * kSortTile; k0 < tileEnd; k0 += blockDim.x) {  // same trip count in every warp
-        const uint32_t k = k0 + threadIdx.x;
-        const bool valid = k < tileEnd;
-        const uint64_t key = valid ? keys[begin + k] : 0;
-        for (int p = 0; p < passes; p++) {
-            const uint32_t d = valid ? static_cast<uint32_t>(key >> (8 * p)) & 0xFF : kNoDigit;
-            const uint32_t peers = __match_any_sync(0xffffffffu, d);
-            if (d != kNoDigit && (peers & lt) == 0) atomicAdd(&h[p][d], static_cast<uint32_t>(__popc(peers)));
+    uint32_t run[8], digit[8];
+#pragma unroll
+    for (int p = 0; p < 8; p++) {
+        run[p] = 0;
+        digit[p] = 0;
+    }
+    for (uint32_t k = local * kSortTile + threadIdx.x; k < tileEnd; k += blockDim.x) {
+        const uint64_t key = keys[begin + k];
+#pragma unroll
+        for (int p = 0; p < 8; p++) {
+            if (p < passes) {
+                const uint32_t d = static_cast<uint32_t>(key >> (8 * p)) & 0xFF;
+                if (d != digit[p]) {
+                    if (run[p]) atomicAdd(&h[p][digit[p]], run[p]);
+                    digit[p] = d;
+                    run[p] = 0;
+                }
+                run[p]++;
+            }
         }
+    }
+#pragma unroll
+    for (int p = 0; p < 8; p++) {
+        if (p < passes && run[p]) atomicAdd(&h[p][digit[p]], run[p]);
     }
     __syncthreads();
     for (int i = threadIdx.x; i < passes * 256; i += blockDim.x) {
