@@ -262,6 +262,8 @@ __global__ void __launch_bounds__(kSortThreads, 3) radixOnesweep(Loader ld, Stor
     Key keys[kSortItems];
     uint32_t rankDigit[kSortItems];  // (rank within warp << 9) | digit
 
+    // Every load of the thread first (all in flight at once), then the ranking: a warp-synchronous
+    // match between two loads would make each load wait for the one before.
 #pragma unroll
     for (int j = 0; j < kSortItems; j++) {
         const uint64_t i = warpBase + j * 32 + lane;
@@ -269,6 +271,11 @@ __global__ void __launch_bounds__(kSortThreads, 3) radixOnesweep(Loader ld, Stor
         if (!(i < count && ld.load(segment, segBegin + static_cast<uint32_t>(i), static_cast<uint32_t>(i), keys[j], d))) {
             d = kNoDigit;
         }
+        rankDigit[j] = d;
+    }
+#pragma unroll
+    for (int j = 0; j < kSortItems; j++) {
+        const uint32_t d = rankDigit[j];
         const uint32_t peers = __match_any_sync(0xffffffffu, d);
         uint32_t before = 0;
         if (d != kNoDigit) before = myCount[d];
@@ -288,20 +295,42 @@ __global__ void __launch_bounds__(kSortThreads, 3) radixOnesweep(Loader ld, Stor
         warpCount[w * 256 + d] = digitTotal;
         digitTotal += c;
     }
-
-    // Publish, then look back for the running total of every earlier tile, four tiles per step
-    // (independent loads), backing off while a predecessor has not published.
+    // Publish the tile's aggregate as early as possible: successors wait on it.
     volatile uint32_t* vs = status;
+    vs[static_cast<size_t>(tile) * 256 + d] = (tile == firstTile ? kStatusPrefix : kStatusAggregate) | digitTotal;
+    uint32_t tileTotal;
+    const uint32_t inclusive = blockInclusiveScan<OpSum>(digitTotal, warpTotals, tileTotal);
+    digitStart[d] = inclusive - digitTotal;
+    __syncthreads();
+
+    // Stage the keys (and every slot's digit) by digit before the look-back, so that the keys leave
+    // the registers, and start the value loads, which complete while the look-back waits.
+    uint32_t vals[kSortItems];
+#pragma unroll
+    for (int j = 0; j < kSortItems; j++) {
+        const uint32_t dj = rankDigit[j] & 0x1FF;
+        vals[j] = 0;
+        if (dj != kNoDigit) {
+            const uint32_t slot = digitStart[dj] + warpCount[warp * 256 + dj] + (rankDigit[j] >> 9);
+            if constexpr (Storer::kKeys) sKeys[slot] = keys[j];
+            sDig[slot] = static_cast<uint8_t>(dj);
+            rankDigit[j] = slot;  // from here on: the item's staged slot
+            const uint64_t i = warpBase + j * 32 + lane;
+            vals[j] = ld.value(segment, segBegin + static_cast<uint32_t>(i), static_cast<uint32_t>(i));
+        } else {
+            rankDigit[j] = 0xFFFFFFFFu;
+        }
+    }
+
+    // Look back for the running total of every earlier tile, kWindow tiles per step (independent
+    // loads), backing off while a predecessor has not published.
     uint32_t exclusive = 0;
-    if (tile == firstTile) {
-        vs[static_cast<size_t>(tile) * 256 + d] = kStatusPrefix | digitTotal;
-    } else {
-        vs[static_cast<size_t>(tile) * 256 + d] = kStatusAggregate | digitTotal;
+    if (tile != firstTile) {
         uint32_t t = tile;
         long long waitStart = -1;
         bool failed = false;
         while (t > firstTile) {
-            constexpr uint32_t kWindow = 4;
+            constexpr uint32_t kWindow = 16;
             const uint32_t avail = min(kWindow, t - firstTile);
             uint32_t w[kWindow];
 #pragma unroll
@@ -339,45 +368,23 @@ __global__ void __launch_bounds__(kSortThreads, 3) radixOnesweep(Loader ld, Stor
         }
     }
     digitGlobal[d] = digitBase[static_cast<size_t>(segment) * 256 + d] + exclusive;
-    uint32_t tileTotal;
-    const uint32_t inclusive = blockInclusiveScan<OpSum>(digitTotal, warpTotals, tileTotal);
-    digitStart[d] = inclusive - digitTotal;
     __syncthreads();
     if (sFailed) {
         if (threadIdx.x == 0) atomicExch(error, 1u);
         return;
     }
 
-    // Staged slot of item j: its digit's start in the tile, the warps before, its rank in the warp.
-    uint32_t slot[kSortItems];
-#pragma unroll
-    for (int j = 0; j < kSortItems; j++) {
-        const uint32_t dj = rankDigit[j] & 0x1FF;
-        slot[j] = dj != kNoDigit ? digitStart[dj] + warpCount[warp * 256 + dj] + (rankDigit[j] >> 9) : 0xFFFFFFFFu;
-    }
     if constexpr (Storer::kKeys) {
-#pragma unroll
-        for (int j = 0; j < kSortItems; j++) {
-            if (slot[j] != 0xFFFFFFFFu) {
-                sKeys[slot[j]] = keys[j];
-                sDig[slot[j]] = static_cast<uint8_t>(rankDigit[j] & 0xFF);
-            }
-        }
-        __syncthreads();
         for (uint32_t i = threadIdx.x; i < tileTotal; i += kSortThreads) {
             const uint32_t dj = sDig[i];
             st.storeKey(segment, digitGlobal[dj] + i - digitStart[dj], sKeys[i]);
         }
         __syncthreads();
     }
-    // Values, derived again by the loader for the same elements, staged in the same buffer.
+    // Values into the same buffer, then out.
 #pragma unroll
     for (int j = 0; j < kSortItems; j++) {
-        if (slot[j] != 0xFFFFFFFFu) {
-            const uint64_t i = warpBase + j * 32 + lane;
-            sVals[slot[j]] = ld.value(segment, segBegin + static_cast<uint32_t>(i), static_cast<uint32_t>(i));
-            if constexpr (!Storer::kKeys) sDig[slot[j]] = static_cast<uint8_t>(rankDigit[j] & 0xFF);
-        }
+        if (rankDigit[j] != 0xFFFFFFFFu) sVals[rankDigit[j]] = vals[j];
     }
     __syncthreads();
     for (uint32_t i = threadIdx.x; i < tileTotal; i += kSortThreads) {
