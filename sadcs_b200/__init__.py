@@ -277,14 +277,17 @@ def rank_sample(text, stats: Stats | None = None) -> np.ndarray:
 
 
 def build(text, want_sa: bool = True, want_bwt: bool = True, context: Context | None = None,
-          stats: Stats | None = None):
-    """SA (uint32) and/or BWT from one construction, host to host, n up to 2^32 - 256.
+          stats: Stats | None = None, out_sa: np.ndarray | None = None, out_bwt: np.ndarray | None = None):
+    """SA (uint32) and/or BWT from one construction, host to host, n up to 2^32 - 256. out_sa /
+    out_bwt may be given as the output buffers (page-locked ones are written by the device directly).
 
     Returns (sa or None, bwt or None, primary or None)."""
     t = _as_text(text)
     n = len(t)
-    sa = np.empty(max(n, 1), np.uint32) if want_sa else None
-    out = np.empty(max(n, 1), np.uint8) if want_bwt else None
+    sa = (out_sa if out_sa is not None else np.empty(max(n, 1), np.uint32)) if want_sa else None
+    out = (out_bwt if out_bwt is not None else np.empty(max(n, 1), np.uint8)) if want_bwt else None
+    if (sa is not None and (sa.dtype != np.uint32 or len(sa) < n)) or (out is not None and (out.dtype != np.uint8 or len(out) < n)):
+        raise ValueError("out_sa must be uint32 and out_bwt uint8, each of at least n entries")
     primary = ctypes.c_int64(-1)
     _check(lib().sadcs_gpu_build(_handle(context), t.ctypes.data_as(_u8p), n,
                                  sa.ctypes.data_as(_u32p) if sa is not None else None,

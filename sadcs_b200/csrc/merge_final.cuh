@@ -187,14 +187,26 @@ __global__ void __launch_bounds__(kMergeThreads) mergeFinal(MergeArgs a) {
     constexpr int kItems = (kMergeCap + kMergeThreads - 1) / kMergeThreads;
     uint32_t p[kItems];
     uint64_t extra[kItems], before[kItems];
+    // Positions first, every list load in flight at once (an asynchronous copy between two loads
+    // would order them), then the records' copies.
 #pragma unroll
     for (int j = 0; j < kItems; j++) {
         const uint32_t e = threadIdx.x + j * kMergeThreads;
         p[j] = 0;
         if (e < size) {
             const int l = listOfElement(t.seg, e);
-            uint32_t q = a.level.lists[st[l] + t.win[l] + (e - t.seg[l])];
-            const uint32_t qEnd = a.texts.endOf(q);
+            p[j] = a.level.lists[st[l] + t.win[l] + (e - t.seg[l])];
+        }
+    }
+    uint32_t ends[kItems];  // the end of each position's text (one load chain per item, all in flight)
+#pragma unroll
+    for (int j = 0; j < kItems; j++) ends[j] = threadIdx.x + j * kMergeThreads < size ? a.texts.endOf(p[j]) : 0;
+#pragma unroll
+    for (int j = 0; j < kItems; j++) {
+        const uint32_t e = threadIdx.x + j * kMergeThreads;
+        if (e < size) {
+            uint32_t q = p[j];
+            const uint32_t qEnd = ends[j];
             if (q >= qEnd) {  // cannot happen for valid class lists; never read out of range
                 atomicExch(a.error, 3u);
                 q = 0;

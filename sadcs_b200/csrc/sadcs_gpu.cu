@@ -339,6 +339,18 @@ int createContext(int64_t capacity, uint32_t texts, sadcs_gpu_context** out) {
     return SADCS_OK;
 }
 
+// The device address of a page-locked host buffer (allocated or registered with CUDA and mapped
+// into the device's address space), or null for pageable memory and null pointers.
+void* mappedHost(void* host) {
+    if (!host) return nullptr;
+    cudaPointerAttributes attributes;
+    if (cudaPointerGetAttributes(&attributes, host) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    return attributes.type == cudaMemoryTypeHost ? attributes.devicePointer : nullptr;
+}
+
 bool isPinned(const void* host) {
     cudaPointerAttributes attributes;
     if (cudaPointerGetAttributes(&attributes, host) != cudaSuccess) {
@@ -743,10 +755,14 @@ int sadcs_gpu_build_batch(sadcs_gpu_context* context, const uint8_t* texts, cons
         io.hostText = texts;
         io.wantSa = sa != nullptr;
         io.wantBwt = bwt != nullptr;
+        // Page-locked outputs are written by the merge itself, over the host link while it runs,
+        // instead of being copied down after it.
+        io.outSa = static_cast<uint32_t*>(mappedHost(sa));
+        io.outBwt = static_cast<uint8_t*>(mappedHost(bwt));
         int status = construct(c, b, io, c->stream, s);
         if (status != SADCS_OK) return status;
-        if (sa && (status = download(c, sa, io.deviceSa, 4 * b.outputs, s)) != SADCS_OK) return status;
-        if (bwt && (status = download(c, bwt, io.deviceBwt, b.outputs, s)) != SADCS_OK) return status;
+        if (sa && !io.outSa && (status = download(c, sa, io.deviceSa, 4 * b.outputs, s)) != SADCS_OK) return status;
+        if (bwt && !io.outBwt && (status = download(c, bwt, io.deviceBwt, b.outputs, s)) != SADCS_OK) return status;
         if (bwt && primaries) {
             std::vector<int64_t> p(b.count);
             if ((status = readPrimaries(c, io, b.count, p.data())) != SADCS_OK) return status;

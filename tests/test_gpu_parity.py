@@ -241,3 +241,22 @@ def test_server_results_equal_alone_and_in_the_mix():
         assert batched > 0  # some requests shared a construction
         constructions, launches = server.counters()
         assert 0 < constructions < len(texts) and launches > 0
+
+
+@pytest.mark.parametrize("n", [1, 2, 100, 70000, 3 << 20])
+def test_page_locked_outputs_written_by_the_device(n):
+    """With page-locked output buffers the merge writes the SA and BWT into host memory directly;
+    the results equal those of the pageable path."""
+    text = W.natural_text(n, seed=31) if n > 100 else W.random_text(W.SplitMix(n), n, 3)
+    ref_sa, ref_bwt, ref_primary = sa.build(text)
+    raw_sa = sa.allocate_pinned(4 * n)
+    raw_bwt = sa.allocate_pinned(n)
+    try:
+        out_sa = raw_sa.view(np.uint32)
+        out_sa[:] = 0xFFFFFFFF
+        raw_bwt[:] = 0
+        got_sa, got_bwt, primary = sa.build(text, out_sa=out_sa, out_bwt=raw_bwt)
+        assert np.array_equal(got_sa, ref_sa) and np.array_equal(got_bwt, ref_bwt) and primary == ref_primary
+    finally:
+        sa.free_pinned(raw_sa)
+        sa.free_pinned(raw_bwt)
