@@ -20,31 +20,37 @@ struct CodeTable {
     uint8_t code[256];
 };
 
-// counts[c] += occurrences of byte c inside the texts (zeroed by the caller).
+// counts[c] += occurrences of byte c inside the texts (zeroed by the caller). Sixteen bytes per
+// thread and iteration (one 16-byte load; the text buffer is 16-byte aligned and padded), counted
+// in one shared histogram per warp so that only lanes of one warp contend for a counter.
 __global__ void __launch_bounds__(256) alphabetHistogram(const uint8_t* __restrict__ text, uint32_t total,
                                                          TextSet texts, uint32_t* __restrict__ counts) {
-    __shared__ uint32_t h[256];
-    h[threadIdx.x] = 0;
+    __shared__ uint32_t h[8][256];
+    for (int i = threadIdx.x; i < 8 * 256; i += blockDim.x) (&h[0][0])[i] = 0;
     __syncthreads();
-    const uint32_t lane = threadIdx.x & 31, lt = (1u << lane) - 1;
-    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x * 4;
-    // The loop runs on the warp's base, so every lane of a warp makes the same number of trips (the
-    // match below names all 32 lanes).
-    for (uint64_t warpBase = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + (threadIdx.x - lane)) * 4;
-         warpBase < total; warpBase += stride) {
-        const uint64_t base = warpBase + lane * 4;
-        const bool any = base < total;
-        const uint32_t word = any ? *reinterpret_cast<const uint32_t*>(text + base) : 0;
-        const uint32_t end = any ? texts.endOf(static_cast<uint32_t>(base)) : 0;
+    uint32_t* mine = h[threadIdx.x >> 5];
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x * 16;
+    for (uint64_t base = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) * 16; base < total;
+         base += stride) {
+        const uint4 v = *reinterpret_cast<const uint4*>(text + base);
+        const uint32_t words[4] = {v.x, v.y, v.z, v.w};
+        if (texts.count <= 1 && base + 16 <= total) {  // one text, all 16 bytes inside it
 #pragma unroll
-        for (int b = 0; b < 4; b++) {
-            const uint32_t c = base + b < end ? (word >> (8 * b)) & 0xFF : 0x100;
-            const uint32_t peers = __match_any_sync(0xffffffffu, c);
-            if (c != 0x100 && (peers & lt) == 0) atomicAdd(&h[c], static_cast<uint32_t>(__popc(peers)));
+            for (int b = 0; b < 16; b++) atomicAdd(&mine[(words[b >> 2] >> (8 * (b & 3))) & 0xFF], 1u);
+        } else {
+            // 16 bytes at a multiple of 16 lie in one 32-byte block, hence in one text's range
+            const uint64_t end = min(static_cast<uint64_t>(total), static_cast<uint64_t>(texts.endOf(static_cast<uint32_t>(base))));
+#pragma unroll
+            for (int b = 0; b < 16; b++) {
+                if (base + b < end) atomicAdd(&mine[(words[b >> 2] >> (8 * (b & 3))) & 0xFF], 1u);
+            }
         }
     }
     __syncthreads();
-    if (h[threadIdx.x]) atomicAdd(counts + threadIdx.x, h[threadIdx.x]);
+    uint32_t sum = 0;
+#pragma unroll
+    for (int w = 0; w < 8; w++) sum += h[w][threadIdx.x];
+    if (sum) atomicAdd(counts + threadIdx.x, sum);
 }
 
 // packed[w] = the 64 bits [64w, 64w + 64) of the code stream. One thread per word; positions past

@@ -137,36 +137,30 @@ struct ClassStorer {
 };
 
 // hist[(d * J + j) * 256 + c] = positions q of text j in class d with code c (zeroed by the caller).
-// Eight characters per thread from one 64-bit read of the code stream.
+// Eight characters per thread from one 64-bit read of the code stream. Consecutive positions are in
+// different classes, so the shared counters of one text rarely collide and plain atomics serve.
 __global__ void __launch_bounds__(256) classHistogram(uint32_t total, TextSet texts, uint32_t* __restrict__ hist) {
     __shared__ uint32_t h[kClasses * 256];
     const bool one = texts.count <= 1;
     for (int i = threadIdx.x; i < kClasses * 256; i += blockDim.x) h[i] = 0;
     __syncthreads();
-    const uint32_t lane = threadIdx.x & 31, lt = (1u << lane) - 1;
     const uint32_t b = texts.bits;
     const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x * 8;
-    // The loop runs on the warp's base, so every lane of a warp makes the same number of trips (the
-    // match below names all 32 lanes).
-    for (uint64_t warpBase = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + (threadIdx.x - lane)) * 8;
-         warpBase < total; warpBase += stride) {
-        const uint64_t base = warpBase + lane * 8;
-        const bool any = base < total;
-        const uint64_t chunk = any ? streamBits(texts.packed, base * b) : 0;
-        const uint32_t j = any ? texts.textOf(static_cast<uint32_t>(base)) : 0;
-        const uint32_t end = any ? texts.endOfText(j) : 0;
+    for (uint64_t base = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) * 8; base < total;
+         base += stride) {
+        const uint64_t chunk = streamBits(texts.packed, base * b);
+        const uint32_t j = texts.textOf(static_cast<uint32_t>(base));
+        const uint32_t end = texts.endOfText(j);
 #pragma unroll
         for (int k = 0; k < 8; k++) {
             const uint64_t q = base + k;
             const uint32_t c = static_cast<uint32_t>(chunk >> (64 - (k + 1) * b)) & ((1u << b) - 1);
             const uint32_t cls = q < end ? cCover.classOf[q % kV] : 0;
-            const uint32_t key = cls ? (cls * texts.count + j) * 256 + c : 0xFFFFFFFFu;
-            const uint32_t peers = __match_any_sync(0xffffffffu, key);
-            if (key != 0xFFFFFFFFu && (peers & lt) == 0) {
+            if (cls) {
                 if (one) {
-                    atomicAdd(&h[key], static_cast<uint32_t>(__popc(peers)));
+                    atomicAdd(&h[cls * 256 + c], 1u);
                 } else {
-                    atomicAdd(hist + key, static_cast<uint32_t>(__popc(peers)));
+                    atomicAdd(hist + (cls * texts.count + j) * 256 + c, 1u);
                 }
             }
         }

@@ -37,7 +37,10 @@ constexpr uint32_t kMergeG = 32;
 #endif
 constexpr uint32_t kMergeR = SADCS_MERGE_R;
 constexpr uint32_t kMergeCap = kMergeG * kMergeR + 6 * (kMergeG - 1) + 1;
-constexpr int kMergeThreads = 256;
+#ifndef SADCS_MERGE_THREADS
+#define SADCS_MERGE_THREADS 256
+#endif
+constexpr int kMergeThreads = SADCS_MERGE_THREADS;  // threads per tile (tuning)
 constexpr int kPairs = kClasses * (kClasses - 1) / 2;
 constexpr uint32_t kNoList = 0xFFFFFFFFu;
 constexpr int kMaxLevels = 10;

@@ -29,6 +29,12 @@ namespace sadcs {
 #define SADCS_MERGE_CARVEOUT 85
 #endif
 
+// Outputs per thread and tree level, at least: each thread's merge-path search is amortised over
+// its chunk (tuning).
+#ifndef SADCS_MERGE_MIN_CHUNK
+#define SADCS_MERGE_MIN_CHUNK 1
+#endif
+
 // 64-bit words of the code stream a final-level record keeps: 31 characters of `bits` bits.
 __host__ __device__ constexpr int finalWords(uint32_t bits) {
     return static_cast<int>((31 * bits + 63) / 64);
@@ -119,7 +125,7 @@ template <int W, bool kMulti>
 __device__ __forceinline__ void finalLevel(const FinalTile<W, kMulti>& s, const uint16_t* src, uint16_t* dst,
                                            const uint32_t* mb, int merges, uint32_t size, uint32_t n,
                                            uint32_t bits) {
-    const uint32_t chunk = (size + kMergeThreads - 1) / kMergeThreads;
+    const uint32_t chunk = max((size + kMergeThreads - 1) / kMergeThreads, static_cast<uint32_t>(SADCS_MERGE_MIN_CHUNK));
     uint32_t at = threadIdx.x * chunk;
     const uint32_t stopAll = min(at + chunk, size);
     int m = 0;

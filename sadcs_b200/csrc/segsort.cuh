@@ -20,6 +20,10 @@
 
 namespace sadcs {
 
+#ifndef SADCS_SEGSORT_BLOCKS
+#define SADCS_SEGSORT_BLOCKS 2  // resident blocks per SM the register budget is set for (tuning)
+#endif
+
 constexpr uint32_t kSegSmall = 2048;                 // largest segment sorted in one block
 constexpr uint32_t kSegChunk = 2048;                 // a block owns the segments starting in such a range
 constexpr uint32_t kSegCap = kSegChunk + kSegSmall;  // elements a block can hold
@@ -161,7 +165,7 @@ __global__ void segCopyBack(ListSegments segs, const uint64_t* __restrict__ kFro
 
 // The small segments starting in [blockIdx.x * kSegChunk, + kSegChunk): sorted by subkey in
 // shared memory and written to out (which may be in). keyBits: significant key bits.
-__global__ void __launch_bounds__(kSegThreads, 2) segSortSmall(const uint32_t* __restrict__ heads, uint32_t segments,
+__global__ void __launch_bounds__(kSegThreads, SADCS_SEGSORT_BLOCKS) segSortSmall(const uint32_t* __restrict__ heads, uint32_t segments,
                                                             const uint64_t* keyIn, const uint32_t* valIn,
                                                             uint64_t* keyOut, uint32_t* valOut, int keyBits) {
     extern __shared__ __align__(16) unsigned char smem[];
