@@ -54,16 +54,20 @@ __global__ void __launch_bounds__(256) alphabetHistogram(const uint8_t* __restri
 }
 
 // packed[w] = the 64 bits [64w, 64w + 64) of the code stream. One thread per word; positions past
-// the end of the concatenation read code 0.
-__global__ void packCodes(const uint8_t* __restrict__ text, uint32_t total, CodeTable table, uint32_t bits,
-                          uint64_t words, uint64_t* __restrict__ packed) {
+// the end of the concatenation read code 0. The byte-to-code table is copied to shared memory
+// first: indexed by data, a kernel-parameter table would serialise a warp's lookups.
+__global__ void __launch_bounds__(256) packCodes(const uint8_t* __restrict__ text, uint32_t total, CodeTable table,
+                                                 uint32_t bits, uint64_t words, uint64_t* __restrict__ packed) {
+    __shared__ uint8_t code[256];
+    code[threadIdx.x] = table.code[threadIdx.x];
+    __syncthreads();
     const uint64_t w = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (w >= words) return;
     const uint64_t firstBit = w * 64;
     const uint64_t first = firstBit / bits, last = (firstBit + 63) / bits;
     uint64_t out = 0;
     for (uint64_t q = first; q <= last; q++) {
-        const uint64_t c = q < total ? table.code[text[q]] : 0;
+        const uint64_t c = q < total ? code[text[q]] : 0;
         // character q spans stream bits [q*bits, q*bits + bits); place it relative to this word
         const int64_t shift = static_cast<int64_t>(firstBit + 64) - static_cast<int64_t>(q * bits + bits);
         out |= shift >= 0 ? (shift < 64 ? c << shift : 0) : c >> (-shift);

@@ -14,14 +14,9 @@
 // which contains every element of b in [s_lo, s_hi), while every element of b before the window is
 // smaller than s_lo. Since sum_b c_b(s) is s's merged position, a window set holds at most
 // G*R + 6*(G-1) + 1 elements whatever the data: one fixed shared-memory capacity, no overflow path.
-// Inside the tile, each of the 21 pairs of windows is merged along a merge path cut into chunks
-// (one diagonal search each, then one comparison per step); the walk records, for each element,
-// how many elements of the other window precede it (each such count is written by exactly one
-// thread, so no atomics). An element's output position is the windows' total start plus its index
-// in its own window plus those counts; the tile writes the elements between s_lo and s_hi.
-//
-// Records (48 bytes, shared memory): the 16 text bytes at p, the 7 sample ranks of [p, p + 32)
-// (all a comparison can need), and p. Comparisons reaching past 16 characters read the text.
+// Inside the tile the windows are merged by a tree of merge paths (merge_final.cuh); an element's
+// output position is the windows' total start plus its rank in the merged window set, and the tile
+// writes the elements between s_lo and s_hi (the last level: SA and BWT; upper levels: rows).
 #pragma once
 
 #include "alphabet.cuh"
@@ -41,7 +36,6 @@ constexpr uint32_t kMergeCap = kMergeG * kMergeR + 6 * (kMergeG - 1) + 1;
 #define SADCS_MERGE_THREADS 256
 #endif
 constexpr int kMergeThreads = SADCS_MERGE_THREADS;  // threads per tile (tuning)
-constexpr int kPairs = kClasses * (kClasses - 1) / 2;
 constexpr uint32_t kNoList = 0xFFFFFFFFu;
 constexpr int kMaxLevels = 10;
 
@@ -50,17 +44,16 @@ struct __align__(16) MergeRow {
     uint32_t c[kClasses];
 };
 
-// w0, w1: 128 bits of the code stream from pos (128 / bits characters); w2 is staging for the
-// third stream word while the record is gathered (see gatherRecord). end: the end of pos's text (texts are ordered by it);
-// text: its index.
-struct __align__(8) MergeRecord {
-    uint64_t w0, w1, w2;
+// A suffix for single comparisons in registers (the searches of mergeSuffixZeroRows): w0, w1 = 128
+// bits of the code stream from pos; end: the end of pos's text (texts are ordered by it); text: its
+// index. Comparisons reaching past w1 read the code stream.
+struct MergeRecord {
+    uint64_t w0, w1;
     uint32_t rank[kK];
     uint32_t pos;
     uint32_t end;
     uint32_t text;
 };
-static_assert(sizeof(MergeRecord) == 64, "record size");
 
 struct MergeLevel {
     const uint32_t* lists;
@@ -159,42 +152,13 @@ __device__ __forceinline__ void cpAsyncWaitAll() {
     asm volatile("cp.async.wait_all;\n" ::: "memory");
 }
 
-// Issues the gather of r's raw text words (the three aligned words covering [p, p + 16)) and its
-// 7 sample ranks as asynchronous copies into shared memory: every load of every record of the
-// thread is in flight at once. finishRecord() turns the raw words into big-endian windows.
-__device__ __forceinline__ void gatherRecord(const uint32_t* __restrict__ ranks, const TextSet& texts, uint32_t p,
-                                             MergeRecord& r) {
-    const uint64_t* words = texts.packed + ((static_cast<uint64_t>(p) * texts.bits) >> 6);
-    cpAsync8(&r.w0, words);
-    cpAsync8(&r.w1, words + 1);
-    cpAsync8(&r.w2, words + 2);
-    const uint32_t* rk = ranks + pack(p);
-#pragma unroll
-    for (int s = 0; s < kK; s++) cpAsync4(&r.rank[s], rk + s);
-    r.pos = p;
-    r.text = texts.textOf(p);
-    r.end = texts.endOfText(r.text);
-}
-
-__device__ __forceinline__ void finishRecord(MergeRecord& r, uint32_t bits) {
-    const uint32_t o = static_cast<uint32_t>((static_cast<uint64_t>(r.pos) * bits) & 63);
-    const uint64_t a = r.w0, b = r.w1, c = r.w2;
-    r.w0 = o ? (a << o) | (b >> (64 - o)) : a;
-    r.w1 = o ? (b << o) | (c >> (64 - o)) : b;
-}
-
 struct MergeTileInfo {
     uint32_t seg[kClasses + 1];
     uint32_t win[kClasses];
-    uint32_t base, loIdx, hiIdx, lrLo, lrHi, size, chunk;
-    uint32_t pairStart[kPairs + 1];
-    uint8_t pairA[kPairs], pairB[kPairs];
+    uint32_t base, loIdx, hiIdx, size;
     int bad;
 };
 
-constexpr size_t mergeSharedBytes() {
-    return kMergeCap * sizeof(MergeRecord) + kMergeCap * 8 * sizeof(uint16_t) + kMergeCap * sizeof(uint32_t);
-}
 
 __device__ __forceinline__ int listOfElement(const uint32_t* seg, uint32_t e) {
     int l = 0;
@@ -251,147 +215,6 @@ __device__ __forceinline__ void planTileWindows(const MergeArgs& a, MergeTileInf
     t.loIdx = loList == kNoList ? kNoList : t.seg[loList];
     t.hiIdx = hiList == kNoList ? kNoList : t.seg[hiList + 1] - 1;
     t.bad = t.size > kMergeCap;
-}
-
-// An upper level's tiles: the rows (every R-th element of the merged order with its per-list counts)
-// that bound the tiles of the level below.
-__global__ void __launch_bounds__(kMergeThreads) mergeTiles(MergeArgs a) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    MergeRecord* rec = reinterpret_cast<MergeRecord*>(smem);
-    uint16_t* cnt = reinterpret_cast<uint16_t*>(rec + kMergeCap);
-    uint32_t* lr = reinterpret_cast<uint32_t*>(cnt + kMergeCap * 8);
-    __shared__ MergeTileInfo t;
-    __shared__ __align__(16) MergeTables tb;
-    {
-        const uint32_t* src = reinterpret_cast<const uint32_t*>(&cCover.tie[0][0]);
-        uint32_t* dst = reinterpret_cast<uint32_t*>(&tb.tie[0][0]);
-        for (int i = threadIdx.x; i < kV * kV / 4; i += kMergeThreads) dst[i] = src[i];
-        const uint32_t* src2 = reinterpret_cast<const uint32_t*>(&cCover.slot[0][0]);
-        uint32_t* dst2 = reinterpret_cast<uint32_t*>(&tb.slot[0][0]);
-        for (int i = threadIdx.x; i < kV * kV / 4; i += kMergeThreads) dst2[i] = src2[i];
-    }
-
-    if (threadIdx.x == 0) {
-        planTileWindows(a, t);
-        const uint32_t steps = (kClasses - 1) * t.size;
-        const uint32_t lanes = kMergeThreads - kPairs;
-        const uint32_t c = max(1u, (steps + lanes - 1) / lanes);
-        uint32_t total = 0;
-        int q = 0;
-        for (int x = 0; x < kClasses; x++) {
-            for (int y = x + 1; y < kClasses; y++, q++) {
-                const uint32_t lenA = t.seg[x + 1] - t.seg[x], lenB = t.seg[y + 1] - t.seg[y];
-                t.pairStart[q] = total;
-                t.pairA[q] = static_cast<uint8_t>(x);
-                t.pairB[q] = static_cast<uint8_t>(y);
-                if (lenA && lenB) total += (lenA + lenB + c - 1) / c;
-            }
-        }
-        t.pairStart[kPairs] = total;
-        t.chunk = c;
-        if (t.bad && a.error) atomicExch(a.error, 1u);
-    }
-    __syncthreads();
-    if (t.bad) return;
-
-    const uint32_t size = t.size;
-    const uint32_t* st = a.level.start;
-    // Positions first (list reads, coalesced), then every record's gather in flight at once.
-    constexpr int kItems = (kMergeCap + kMergeThreads - 1) / kMergeThreads;
-    uint32_t pos[kItems];
-#pragma unroll
-    for (int j = 0; j < kItems; j++) {
-        const uint32_t e = threadIdx.x + j * kMergeThreads;
-        pos[j] = 0;
-        if (e < size) {
-            const int l = listOfElement(t.seg, e);
-            uint32_t p = a.level.lists[st[l] + t.win[l] + (e - t.seg[l])];
-            if (p >= a.texts.endOf(p)) {  // cannot happen for valid class lists; never read out of range
-                atomicExch(a.error, 3u);
-                p = 0;
-            }
-            pos[j] = p;
-        }
-    }
-#pragma unroll
-    for (int j = 0; j < kItems; j++) {
-        const uint32_t e = threadIdx.x + j * kMergeThreads;
-        if (e < size) gatherRecord(a.ranks, a.texts, pos[j], rec[e]);
-    }
-    uint32_t* cnt32 = reinterpret_cast<uint32_t*>(cnt);
-    for (uint32_t i = threadIdx.x; i < size * 4; i += kMergeThreads) cnt32[i] = 0;
-    cpAsyncWaitAll();
-#pragma unroll
-    for (int j = 0; j < kItems; j++) {
-        const uint32_t e = threadIdx.x + j * kMergeThreads;
-        if (e < size) finishRecord(rec[e], a.texts.bits);
-    }
-    __syncthreads();
-
-    const uint32_t items = t.pairStart[kPairs], c = t.chunk;
-    for (uint32_t item = threadIdx.x; item < items; item += kMergeThreads) {
-        int q = 0;
-        while (item >= t.pairStart[q + 1]) q++;
-        const uint32_t la = t.pairA[q], lb = t.pairB[q];
-        const uint32_t sa = t.seg[la], lenA = t.seg[la + 1] - sa;
-        const uint32_t sb = t.seg[lb], lenB = t.seg[lb + 1] - sb;
-        uint32_t d = (item - t.pairStart[q]) * c;
-        const uint32_t end = min(d + c, lenA + lenB);
-        uint32_t lo = d > lenB ? d - lenB : 0, hi = min(d, lenA);
-        while (lo < hi) {
-            const uint32_t mid = (lo + hi) >> 1;
-            if (lessRecord(rec[sa + mid], rec[sb + d - 1 - mid], a.texts, tb)) {
-                lo = mid + 1;
-            } else {
-                hi = mid;
-            }
-        }
-        uint32_t i = lo, j = d - lo;
-        for (; d < end; d++) {
-            if (j == lenB || (i < lenA && lessRecord(rec[sa + i], rec[sb + j], a.texts, tb))) {
-                cnt[(sa + i) * 8 + lb] = static_cast<uint16_t>(j);
-                i++;
-            } else {
-                cnt[(sb + j) * 8 + la] = static_cast<uint16_t>(i);
-                j++;
-            }
-        }
-    }
-    __syncthreads();
-
-    for (uint32_t e = threadIdx.x; e < size; e += kMergeThreads) {
-        const int l = listOfElement(t.seg, e);
-        uint32_t r = e - t.seg[l];
-#pragma unroll
-        for (int b = 0; b < kClasses; b++) r += b == l ? 0u : cnt[e * 8 + b];
-        lr[e] = r;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        t.lrLo = t.loIdx == kNoList ? 0 : lr[t.loIdx];
-        t.lrHi = t.hiIdx == kNoList ? size : lr[t.hiIdx];
-    }
-    __syncthreads();
-
-    for (uint32_t e = threadIdx.x; e < size; e += kMergeThreads) {
-        const uint32_t r = lr[e];
-        if (r < t.lrLo || r >= t.lrHi) continue;
-        const uint32_t g = t.base + r;
-        if (g >= a.level.start[kClasses]) {  // cannot happen for a correct tiling; never write out of range
-            atomicExch(a.error, 2u);
-            continue;
-        }
-        if (g % kMergeR == 0) {
-            const int l = listOfElement(t.seg, e);
-            MergeRow row;
-            row.list = static_cast<uint32_t>(l);
-#pragma unroll
-            for (int b = 0; b < kClasses; b++) {
-                row.c[b] = b == l ? t.win[l] + (e - t.seg[l]) : t.win[b] + cnt[e * 8 + b];
-            }
-            a.rowsOut[g / kMergeR] = row;
-        }
-    }
 }
 
 // S_{L+1}: every G-th element of each list of level L.
@@ -487,8 +310,9 @@ inline MergePlan planMerge(const uint32_t* classStart) {
     return p;
 }
 
-// The final level (merge_final.cuh).
-inline cudaError_t launchFinal(const MergeArgs& args, uint32_t tiles, cudaStream_t stream);
+// The merge levels (merge_final.cuh).
+template <bool kFinal>
+inline cudaError_t launchTree(const MergeArgs& args, uint32_t tiles, cudaStream_t stream);
 
 // Merges the class lists of the texts into sa and/or bwt (either may be null). splitters and rows
 // are scratch sized by planMerge; counter is one device word (scratch); rowZero and outBase are per
@@ -498,14 +322,6 @@ inline cudaError_t mergeClasses(const uint8_t* text, const uint32_t* ranks, cons
                                 uint32_t* rowZero, uint32_t* splitters, MergeRow* rows, uint32_t* sa, uint8_t* bwt,
                                 uint32_t* counter, uint32_t* hostWord, cudaStream_t stream,
                                 cudaEvent_t finalStart = nullptr, cudaEvent_t finalStop = nullptr) {
-    static uint64_t configured = 0;
-    int device = 0;
-    SADCS_TRY(cudaGetDevice(&device));
-    if (!(configured >> (device & 63) & 1)) {
-        SADCS_TRY(cudaFuncSetAttribute(mergeTiles, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       static_cast<int>(mergeSharedBytes())));
-        configured |= uint64_t(1) << (device & 63);
-    }
     MergeLevel level[kMaxLevels];
     for (int L = 0; L <= plan.top; L++) {
         level[L].lists = L == 0 ? lists : splitters + plan.listWord[L];
@@ -540,13 +356,13 @@ inline cudaError_t mergeClasses(const uint8_t* text, const uint32_t* ranks, cons
             args.sa = sa;
             args.bwt = bwt;
             if (finalStart) SADCS_TRY(cudaEventRecord(finalStart, stream));
-            SADCS_TRY(launchFinal(args, tiles, stream));
+            SADCS_TRY(launchTree<true>(args, tiles, stream));
             if (finalStop) SADCS_TRY(cudaEventRecord(finalStop, stream));
         } else {
             args.rowsOut = rows + plan.rowIndex[L - 1];
             SADCS_TRY(launch(mergeWriteSentinel, 1, 32, 0, stream, rows + plan.rowIndex[L - 1] + plan.tiles[L - 1],
                              level[L]));
-            SADCS_TRY(launch(mergeTiles, tiles, kMergeThreads, mergeSharedBytes(), stream, args));
+            SADCS_TRY(launchTree<false>(args, tiles, stream));
         }
     }
     SADCS_TRY(cudaMemcpyAsync(hostWord, counter, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));

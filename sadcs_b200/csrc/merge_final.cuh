@@ -1,5 +1,5 @@
-// merge_final.cuh - the last merge level: every tile of the 7 class lists merged in shared memory and
-// written as the suffix array and the BWT.
+// merge_final.cuh - the merge levels: every tile of the 7 lists of a level merged in shared memory;
+// the last level writes the suffix array and the BWT, an upper level the rows of the level below.
 //
 // A tile's window set (at most kMergeCap records, merge.cuh) is held as arrays of fields, not as
 // records, so the 32 threads of a warp reading one field of 32 records hit 32 different banks:
@@ -163,8 +163,10 @@ __device__ __forceinline__ void finalLevel(const FinalTile<W, kMulti>& s, const 
     }
 }
 
-template <int W, bool kMulti>
-__global__ void __launch_bounds__(kMergeThreads) mergeFinal(MergeArgs a) {
+// kFinal: the last level, writing the SA and the BWT; otherwise an upper level, writing the rows
+// (every R-th element of the merged order with its per-list counts) that bound the tiles below.
+template <int W, bool kMulti, bool kFinal>
+__global__ void __launch_bounds__(kMergeThreads) mergeTree(MergeArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     FinalTile<W, kMulti> s;
     s.carve(smem);
@@ -238,7 +240,7 @@ __global__ void __launch_bounds__(kMergeThreads) mergeFinal(MergeArgs a) {
             const uint64_t bit = static_cast<uint64_t>(p[j]) * bits;
             const uint64_t w0 = bit >> 6;
             extra[j] = __ldg(a.texts.packed + w0 + W);
-            if ((bit & 63) < bits && w0 > 0) before[j] = __ldg(a.texts.packed + w0 - 1);
+            if (kFinal && (bit & 63) < bits && w0 > 0) before[j] = __ldg(a.texts.packed + w0 - 1);
         }
     }
     cpAsyncWaitAll();
@@ -252,8 +254,10 @@ __global__ void __launch_bounds__(kMergeThreads) mergeFinal(MergeArgs a) {
             for (int w = 0; w < W; w++) r[w] = s.words[w * kMergeCap + e];
             r[W] = extra[j];
             // the character before p ends at bit o of word 0: bits [64 + o - b, 64 + o) of before:r[0]
-            const uint64_t window = o ? (before[j] << o) | (r[0] >> (64 - o)) : before[j];
-            s.prev[e] = static_cast<uint8_t>(window & ((1u << bits) - 1));
+            if constexpr (kFinal) {
+                const uint64_t window = o ? (before[j] << o) | (r[0] >> (64 - o)) : before[j];
+                s.prev[e] = static_cast<uint8_t>(window & ((1u << bits) - 1));
+            }
             if (o) {
 #pragma unroll
                 for (int w = 0; w < W; w++) s.words[w * kMergeCap + e] = (r[w] << o) | (r[w + 1] >> (64 - o));
@@ -279,57 +283,94 @@ __global__ void __launch_bounds__(kMergeThreads) mergeFinal(MergeArgs a) {
     }
     __syncthreads();
     const uint32_t lo = sLo, hi = sHi;
-    for (uint32_t r = lo + threadIdx.x; r < hi; r += kMergeThreads) {
-        const uint32_t x = order[r];
-        const uint32_t q = s.pos[x];
-        const uint32_t gIdx = t.base + r;
-        if (gIdx >= a.level.start[kClasses]) {  // cannot happen for a correct tiling; never write out of range
-            atomicExch(a.error, 2u);
-            continue;
+    if constexpr (kFinal) {
+        for (uint32_t r = lo + threadIdx.x; r < hi; r += kMergeThreads) {
+            const uint32_t x = order[r];
+            const uint32_t q = s.pos[x];
+            const uint32_t gIdx = t.base + r;
+            if (gIdx >= a.level.start[kClasses]) {  // cannot happen for a correct tiling; never write out of range
+                atomicExch(a.error, 2u);
+                continue;
+            }
+            const uint32_t tj = kMulti ? a.texts.textOf(q) : 0;
+            const uint32_t first = kMulti ? a.texts.startOf(tj) : 0;
+            if (a.sa) a.sa[gIdx] = q - first;
+            if (a.bwt && q != first) {
+                const uint32_t base = kMulti ? __ldg(a.outBase + tj) : 0;
+                const uint32_t row = gIdx - base, zero = __ldg(a.rowZero + tj);
+                a.bwt[base + (row < zero ? row + 1 : row)] = __ldg(a.texts.decode + s.prev[x]);
+            }
         }
-        const uint32_t tj = kMulti ? a.texts.textOf(q) : 0;
-        const uint32_t first = kMulti ? a.texts.startOf(tj) : 0;
-        if (a.sa) a.sa[gIdx] = q - first;
-        if (a.bwt && q != first) {
-            const uint32_t base = kMulti ? __ldg(a.outBase + tj) : 0;
-            const uint32_t row = gIdx - base, zero = __ldg(a.rowZero + tj);
-            a.bwt[base + (row < zero ? row + 1 : row)] = __ldg(a.texts.decode + s.prev[x]);
+    } else {
+        // rank[x] of every record in the merged order (idxA is free again), then the rows: for a
+        // sampled element, the elements of each other list before it are those of its window with a
+        // smaller rank (a binary search: each window is in list order, hence in rank order).
+        uint16_t* rank = s.idxA;
+        for (uint32_t r = threadIdx.x; r < size; r += kMergeThreads) rank[order[r]] = static_cast<uint16_t>(r);
+        __syncthreads();
+        for (uint32_t r = lo + threadIdx.x; r < hi; r += kMergeThreads) {
+            const uint32_t g = t.base + r;
+            if (g % kMergeR != 0) continue;
+            if (g >= a.level.start[kClasses]) {  // cannot happen for a correct tiling; never write out of range
+                atomicExch(a.error, 2u);
+                continue;
+            }
+            const uint32_t x = order[r];
+            const int l = listOfElement(t.seg, x);
+            MergeRow row;
+            row.list = static_cast<uint32_t>(l);
+#pragma unroll
+            for (int b = 0; b < kClasses; b++) {
+                if (b == l) {
+                    row.c[b] = t.win[l] + (x - t.seg[l]);
+                    continue;
+                }
+                uint32_t from = t.seg[b], to = t.seg[b + 1];  // first record of list b ranked at or after r
+                while (from < to) {
+                    const uint32_t mid = (from + to) >> 1;
+                    if (rank[mid] < r) from = mid + 1; else to = mid;
+                }
+                row.c[b] = t.win[b] + (from - t.seg[b]);
+            }
+            a.rowsOut[g / kMergeR] = row;
         }
     }
 }
 
-// Launches the final level for the texts' code width (W words per record) and text count.
-template <int W, bool kMulti>
-inline cudaError_t launchFinalFor(const MergeArgs& args, uint32_t tiles, cudaStream_t stream) {
+// Launches a level (kFinal: the last) for the texts' code width (W words per record) and text count.
+template <int W, bool kMulti, bool kFinal>
+inline cudaError_t launchTreeFor(const MergeArgs& args, uint32_t tiles, cudaStream_t stream) {
     constexpr size_t shared = FinalTile<W, kMulti>::sharedBytes();
     static uint64_t configured = 0;
     int device = 0;
     SADCS_TRY(cudaGetDevice(&device));
     if (!(configured >> (device & 63) & 1)) {
-        SADCS_TRY(cudaFuncSetAttribute(mergeFinal<W, kMulti>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        SADCS_TRY(cudaFuncSetAttribute(mergeTree<W, kMulti, kFinal>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(shared)));
 #if SADCS_MERGE_CARVEOUT >= 0
-        SADCS_TRY(cudaFuncSetAttribute(mergeFinal<W, kMulti>, cudaFuncAttributePreferredSharedMemoryCarveout,
+        SADCS_TRY(cudaFuncSetAttribute(mergeTree<W, kMulti, kFinal>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                        SADCS_MERGE_CARVEOUT));
 #endif
         configured |= uint64_t(1) << (device & 63);
     }
-    return launch(mergeFinal<W, kMulti>, tiles, kMergeThreads, shared, stream, args);
+    return launch(mergeTree<W, kMulti, kFinal>, tiles, kMergeThreads, shared, stream, args);
 }
 
-template <bool kMulti>
-inline cudaError_t launchFinalMulti(const MergeArgs& args, uint32_t tiles, cudaStream_t stream) {
+template <bool kMulti, bool kFinal>
+inline cudaError_t launchTreeWidth(const MergeArgs& args, uint32_t tiles, cudaStream_t stream) {
     switch (finalWords(args.texts.bits)) {
-        case 1: return launchFinalFor<1, kMulti>(args, tiles, stream);
-        case 2: return launchFinalFor<2, kMulti>(args, tiles, stream);
-        case 3: return launchFinalFor<3, kMulti>(args, tiles, stream);
-        default: return launchFinalFor<4, kMulti>(args, tiles, stream);
+        case 1: return launchTreeFor<1, kMulti, kFinal>(args, tiles, stream);
+        case 2: return launchTreeFor<2, kMulti, kFinal>(args, tiles, stream);
+        case 3: return launchTreeFor<3, kMulti, kFinal>(args, tiles, stream);
+        default: return launchTreeFor<4, kMulti, kFinal>(args, tiles, stream);
     }
 }
 
-inline cudaError_t launchFinal(const MergeArgs& args, uint32_t tiles, cudaStream_t stream) {
-    return args.texts.count > 1 ? launchFinalMulti<true>(args, tiles, stream)
-                                : launchFinalMulti<false>(args, tiles, stream);
+// One merge level: kFinal writes the SA and BWT, otherwise the rows of the level below.
+template <bool kFinal>
+inline cudaError_t launchTree(const MergeArgs& args, uint32_t tiles, cudaStream_t stream) {
+    return args.texts.count > 1 ? launchTreeWidth<true, kFinal>(args, tiles, stream)
+                                : launchTreeWidth<false, kFinal>(args, tiles, stream);
 }
 
 }  // namespace sadcs
