@@ -204,23 +204,62 @@ Layout planLayout(const Extent& x, bool internalSa, bool internalBwt) {
     return L;
 }
 
-// Copies the packed texts (text j at packedOffset[j]) to their 32-aligned places and zeroes every
-// gap and the padding after the last text. One block per text.
-__global__ void placeTexts(const uint8_t* __restrict__ packed, const uint32_t* __restrict__ start,
-                           const uint32_t* __restrict__ end, const uint32_t* __restrict__ packedOffset, uint32_t count,
-                           uint32_t span, uint8_t* __restrict__ text) {
-    const uint32_t j = blockIdx.x;
-    const uint32_t s = start[j], e = end[j], next = j + 1 < count ? start[j + 1] : span + kTextPad;
-    const uint8_t* src = packed + packedOffset[j];
-    for (uint32_t i = s + threadIdx.x; i < next; i += blockDim.x) text[i] = i < e ? src[i - s] : 0;
+// The text whose packed range [packedOffset[j], packedOffset[j + 1]) holds packed byte s (binary
+// search; packedOffset has count + 1 entries).
+__device__ __forceinline__ uint32_t packedTextOf(const uint32_t* __restrict__ packedOffset, uint32_t count, uint64_t s) {
+    uint32_t lo = 0, hi = count;  // last j with packedOffset[j] <= s
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (__ldg(packedOffset + mid) <= s) lo = mid; else hi = mid;
+    }
+    return lo;
 }
 
-// blockText[k] = the text whose range contains or precedes the 32-byte block k. One block per text.
-__global__ void fillBlockText(const uint32_t* __restrict__ start, uint32_t count, uint32_t span,
+// Copies the packed texts (text j at packedOffset[j]) to their 32-aligned places. Each thread moves
+// 16 packed bytes (one aligned load) to their text's place, finding the text once per piece (again
+// when the piece crosses into the next text). Gaps are zeroed by placeGaps.
+__global__ void placeTexts(const uint8_t* __restrict__ packed, const uint32_t* __restrict__ start,
+                           const uint32_t* __restrict__ packedOffset, uint32_t count, uint64_t outputs,
+                           uint8_t* __restrict__ text) {
+    const uint64_t s0 = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) * 16;
+    if (s0 >= outputs) return;
+    const uint4 v = *reinterpret_cast<const uint4*>(packed + s0);
+    const uint32_t words[4] = {v.x, v.y, v.z, v.w};
+    uint32_t j = packedTextOf(packedOffset, count, s0);
+    uint32_t next = __ldg(packedOffset + j + 1);
+#pragma unroll
+    for (int b = 0; b < 16; b++) {
+        const uint64_t s = s0 + b;
+        if (s >= outputs) break;
+        while (s >= next) {  // crossed into the next text (empty texts are not in a batch)
+            j++;
+            next = __ldg(packedOffset + j + 1);
+        }
+        text[__ldg(start + j) + (s - __ldg(packedOffset + j))] = static_cast<uint8_t>(words[b >> 2] >> (8 * (b & 3)));
+    }
+}
+
+// Zeroes the gap after every text (up to the next 32-aligned start) and the padding after the last.
+__global__ void placeGaps(const uint32_t* __restrict__ start, const uint32_t* __restrict__ end, uint32_t count,
+                          uint32_t span, uint8_t* __restrict__ text) {
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= count) return;
+    const uint32_t next = j + 1 < count ? start[j + 1] : span + kTextPad;
+    for (uint32_t i = end[j]; i < next; i++) text[i] = 0;
+}
+
+// blockText[k] = the text whose range contains or precedes the 32-byte block k (k = 0 .. span / 32).
+__global__ void fillBlockText(const uint32_t* __restrict__ start, uint32_t count, uint32_t blocks,
                               uint32_t* __restrict__ blockText) {
-    const uint32_t j = blockIdx.x;
-    const uint32_t first = start[j] / kV, last = (j + 1 < count ? start[j + 1] : span) / kV + (j + 1 < count ? 0 : 1);
-    for (uint32_t k = first + threadIdx.x; k < last; k += blockDim.x) blockText[k] = j;
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k > blocks) return;
+    const uint32_t p = k * kV;
+    uint32_t lo = 0, hi = count;  // last j with start[j] <= p
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (__ldg(start + mid) <= p) lo = mid; else hi = mid;
+    }
+    blockText[k] = lo;
 }
 
 }  // namespace
@@ -491,13 +530,16 @@ int construct(sadcs_gpu_context* c, const Batch& b, Io& io, cudaStream_t stream,
                                             stream)) != cudaSuccess) {
             return failed("upload", error);
         }
-        if ((error = cudaMemcpyAsync(packedOffset, dOutBase, 4 * static_cast<size_t>(J), cudaMemcpyDeviceToDevice,
+        if ((error = cudaMemcpyAsync(packedOffset, dOutBase, 4 * (static_cast<size_t>(J) + 1), cudaMemcpyDeviceToDevice,
                                      stream)) != cudaSuccess) {
             return failed("upload", error);
         }
-        if ((error = launch(placeTexts, J, 256, 0, stream, staging, dStart, dEnd, packedOffset, J,
-                            static_cast<uint32_t>(b.span), text)) != cudaSuccess ||
-            (error = launch(fillBlockText, J, 256, 0, stream, dStart, J, static_cast<uint32_t>(b.span), dBlockText)) !=
+        const uint32_t blocks = static_cast<uint32_t>(b.span / kV);
+        if ((error = launch(placeTexts, ceilDiv(ceilDiv(b.outputs, 16), 256), 256, 0, stream, staging, dStart, packedOffset,
+                            J, b.outputs, text)) != cudaSuccess ||
+            (error = launch(placeGaps, ceilDiv(J, 256), 256, 0, stream, dStart, dEnd, J, static_cast<uint32_t>(b.span),
+                            text)) != cudaSuccess ||
+            (error = launch(fillBlockText, ceilDiv(blocks + 1ull, 256), 256, 0, stream, dStart, J, blocks, dBlockText)) !=
                 cudaSuccess) {
             return failed("placing the texts", error);
         }

@@ -36,6 +36,15 @@ struct ServerRequest {
     bool done = false;
 };
 
+// SADCS_SERVER_TRACE=1 in the environment: one line per construction on stderr.
+bool serverTraceEnabled() {
+    static const bool enabled = [] {
+        const char* v = std::getenv("SADCS_SERVER_TRACE");
+        return v && v[0] && v[0] != '0';
+    }();
+    return enabled;
+}
+
 double nowSeconds() {
     return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
@@ -73,6 +82,7 @@ void serveBatch(sadcs_gpu_server* srv, sadcs_gpu_context& ctx, std::vector<Serve
     int status = SADCS_OK;
     std::string message;
     const double started = nowSeconds();
+    double constructed = started;
     for (ServerRequest* r : group) r->started = started;
     cudaError_t error = cudaMallocFromPoolAsync(reinterpret_cast<void**>(&ctx.slab), footprint, srv->pool, ctx.stream);
     if (error != cudaSuccess) {
@@ -90,6 +100,9 @@ void serveBatch(sadcs_gpu_server* srv, sadcs_gpu_context& ctx, std::vector<Serve
         std::vector<const uint8_t*> pieces;
         if (group.size() == 1) {
             io.hostText = group[0]->text;
+            // Page-locked outputs are written by the merge itself (see sadcs_gpu_build_batch).
+            io.outSa = static_cast<uint32_t*>(mappedHost(group[0]->sa));
+            io.outBwt = static_cast<uint8_t*>(mappedHost(group[0]->bwt));
         } else {
             // Each request's text goes straight from the caller's buffer into the device staging
             // region (asynchronous from page-locked memory; the driver stages pageable memory).
@@ -97,13 +110,14 @@ void serveBatch(sadcs_gpu_server* srv, sadcs_gpu_context& ctx, std::vector<Serve
             io.hostPieces = pieces.data();
         }
         status = construct(&ctx, b, io, ctx.stream, stats);
+        constructed = nowSeconds();
         if (status == SADCS_OK) {
             uint64_t offset = 0;
             for (ServerRequest* r : group) {
-                if ((error = cudaMemcpyAsync(r->sa, io.deviceSa + offset, 4 * r->n, cudaMemcpyDeviceToHost,
-                                             ctx.stream)) != cudaSuccess ||
-                    (error = cudaMemcpyAsync(r->bwt, io.deviceBwt + offset, r->n, cudaMemcpyDeviceToHost,
-                                             ctx.stream)) != cudaSuccess) {
+                if ((!io.outSa && (error = cudaMemcpyAsync(r->sa, io.deviceSa + offset, 4 * r->n,
+                                                           cudaMemcpyDeviceToHost, ctx.stream)) != cudaSuccess) ||
+                    (!io.outBwt && (error = cudaMemcpyAsync(r->bwt, io.deviceBwt + offset, r->n,
+                                                            cudaMemcpyDeviceToHost, ctx.stream)) != cudaSuccess)) {
                     status = failed("download", error);
                     break;
                 }
@@ -121,6 +135,11 @@ void serveBatch(sadcs_gpu_server* srv, sadcs_gpu_context& ctx, std::vector<Serve
         cudaStreamSynchronize(ctx.stream);
     }
     const double done = nowSeconds();
+    if (serverTraceEnabled()) {
+        fprintf(stderr, "sadcs server: %zu texts, %.1f MiB: %.3f s (device %.3f, upload %.3f, after %.3f)\n",
+                group.size(), b.outputs / 1048576.0, done - started, stats.device_seconds, stats.upload_seconds,
+                done - constructed);
+    }
     std::lock_guard<std::mutex> lock(srv->mu);
     srv->inUse -= footprint;
     srv->launches += static_cast<uint64_t>(stats.kernel_launches);
