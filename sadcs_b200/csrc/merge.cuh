@@ -71,6 +71,8 @@ struct MergeArgs {
     MergeRow* rowsOut;       // levels >= 1
     uint32_t* sa;            // level 0, optional: text-local positions
     uint8_t* bwt;            // level 0, optional: the final BWT bytes of every text
+    uint32_t* const* saTexts;  // level 0, optional, in place of sa: one output array per text
+    uint8_t* const* bwtTexts;  // level 0, optional, in place of bwt: one output array per text
     uint32_t* error;         // set nonzero if a window set exceeds the capacity (never, by construction)
 };
 
@@ -271,9 +273,15 @@ __global__ void mergeSuffixZeroRows(MergeArgs a, const uint32_t* __restrict__ ro
 
 // bwt[outBase[j]] = the last character of text j (the sentinel's row).
 __global__ void mergeBwtHeads(const uint8_t* __restrict__ text, TextSet texts, const uint32_t* __restrict__ outBase,
-                              uint8_t* bwt) {
+                              uint8_t* bwt, uint8_t* const* bwtTexts) {
     const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j < texts.count) bwt[outBase[j]] = charByte(texts, texts.endOfText(j) - 1);
+    if (j >= texts.count) return;
+    const uint8_t c = charByte(texts, texts.endOfText(j) - 1);
+    if (bwtTexts) {
+        bwtTexts[j][0] = c;
+    } else {
+        bwt[outBase[j]] = c;
+    }
 }
 
 // Sizes of every level, planned on the host from n alone.
@@ -321,7 +329,8 @@ inline cudaError_t mergeClasses(const uint8_t* text, const uint32_t* ranks, cons
                                 const MergePlan& plan, const uint32_t* rowBase, const uint32_t* outBase,
                                 uint32_t* rowZero, uint32_t* splitters, MergeRow* rows, uint32_t* sa, uint8_t* bwt,
                                 uint32_t* counter, uint32_t* hostWord, cudaStream_t stream,
-                                cudaEvent_t finalStart = nullptr, cudaEvent_t finalStop = nullptr) {
+                                cudaEvent_t finalStart = nullptr, cudaEvent_t finalStop = nullptr,
+                                uint32_t* const* saTexts = nullptr, uint8_t* const* bwtTexts = nullptr) {
     MergeLevel level[kMaxLevels];
     for (int L = 0; L <= plan.top; L++) {
         level[L].lists = L == 0 ? lists : splitters + plan.listWord[L];
@@ -340,12 +349,14 @@ inline cudaError_t mergeClasses(const uint8_t* text, const uint32_t* ranks, cons
     base.outBase = outBase;
     base.rowZero = rowZero;
     base.error = counter;
-    if (bwt) {
+    base.saTexts = saTexts;
+    base.bwtTexts = bwtTexts;
+    if (bwt || bwtTexts) {
         MergeArgs z = base;
         z.level = level[0];
         SADCS_TRY(cudaMemsetAsync(rowZero, 0, sizeof(uint32_t) * texts.count, stream));
         SADCS_TRY(launch(mergeSuffixZeroRows, texts.count, 32, 0, stream, z, rowBase, level[0], rowZero));
-        SADCS_TRY(launch(mergeBwtHeads, (texts.count + 255) / 256, 256, 0, stream, text, texts, outBase, bwt));
+        SADCS_TRY(launch(mergeBwtHeads, (texts.count + 255) / 256, 256, 0, stream, text, texts, outBase, bwt, bwtTexts));
     }
     for (int L = plan.top; L >= 0; L--) {
         MergeArgs args = base;

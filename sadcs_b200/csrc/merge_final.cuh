@@ -294,11 +294,21 @@ __global__ void __launch_bounds__(kMergeThreads) mergeTree(MergeArgs a) {
             }
             const uint32_t tj = kMulti ? a.texts.textOf(q) : 0;
             const uint32_t first = kMulti ? a.texts.startOf(tj) : 0;
-            if (a.sa) a.sa[gIdx] = q - first;
-            if (a.bwt && q != first) {
-                const uint32_t base = kMulti ? __ldg(a.outBase + tj) : 0;
+            const uint32_t base = kMulti ? __ldg(a.outBase + tj) : 0;
+            if (kMulti && a.saTexts) {
+                a.saTexts[tj][gIdx - base] = q - first;
+            } else if (a.sa) {
+                a.sa[gIdx] = q - first;
+            }
+            if ((a.bwt || (kMulti && a.bwtTexts)) && q != first) {
                 const uint32_t row = gIdx - base, zero = __ldg(a.rowZero + tj);
-                a.bwt[base + (row < zero ? row + 1 : row)] = __ldg(a.texts.decode + s.prev[x]);
+                const uint32_t local = row < zero ? row + 1 : row;
+                const uint8_t c = __ldg(a.texts.decode + s.prev[x]);
+                if (kMulti && a.bwtTexts) {
+                    a.bwtTexts[tj][local] = c;
+                } else {
+                    a.bwt[base + local] = c;
+                }
             }
         }
     } else {

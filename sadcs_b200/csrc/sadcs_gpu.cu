@@ -110,7 +110,8 @@ bool planBatch(const uint64_t* lengths, uint32_t count, Batch& b) {
 // Words of the per-construction tables: start, end, sampleBase, outBase, rowZero, the class
 // tables and (several texts) the text of every 32-byte block.
 size_t metaWords(uint32_t count, uint64_t span) {
-    return 5 * static_cast<size_t>(count) + 1 + ClassTables::words(count) + (count > 1 ? span / kV + 1 : 0) + 16;
+    return 5 * static_cast<size_t>(count) + 1 + ClassTables::words(count) + (count > 1 ? span / kV + 1 : 0) + 16 +
+           4 * static_cast<size_t>(count) + 2;  // + the per-text output pointer tables (8-byte aligned)
 }
 
 // Byte offsets of every buffer of a construction, and the peaks.
@@ -445,6 +446,8 @@ struct Io {
     const uint8_t* hostText = nullptr;    // packed host texts, or
     const uint8_t* deviceText = nullptr;  // packed device texts, or
     const uint8_t* const* hostPieces = nullptr;  // one host buffer per text (a batch of several)
+    uint32_t* const* saPieces = nullptr;  // device-accessible outputs, one per text (a batch of several),
+    uint8_t* const* bwtPieces = nullptr;  // in place of outSa / outBwt
     bool wantSa = false, wantBwt = false;
     uint32_t* outSa = nullptr;            // device outputs (caller-owned), or null for the slab's
     uint8_t* outBwt = nullptr;
@@ -462,7 +465,8 @@ int construct(sadcs_gpu_context* c, const Batch& b, Io& io, cudaStream_t stream,
                  c->maxTexts);
         return SADCS_NOT_ENOUGH_MEMORY;
     }
-    const Layout L = planLayout(extentOf(b), io.wantSa && !io.outSa, io.wantBwt && !io.outBwt);
+    const Layout L = planLayout(extentOf(b), io.wantSa && !io.outSa && !io.saPieces,
+                                io.wantBwt && !io.outBwt && !io.bwtPieces);
     if (L.peak > c->slabBytes) {
         setError("internal: layout of %llu bytes exceeds the slab of %llu", static_cast<unsigned long long>(L.peak),
                  static_cast<unsigned long long>(c->slabBytes));
@@ -481,6 +485,8 @@ int construct(sadcs_gpu_context* c, const Batch& b, Io& io, cudaStream_t stream,
     uint32_t* dRowZero = dOutBase + J + 1;
     uint32_t* dClassTables = dRowZero + J;
     uint32_t* dBlockText = dClassTables + ClassTables::words(J);
+    uint32_t* tablesEnd = dBlockText + (J > 1 ? b.span / kV + 1 : 0);
+    uint64_t* dPieces = reinterpret_cast<uint64_t*>(tablesEnd + ((tablesEnd - meta) & 1));  // [sa J][bwt J]
     ClassTables classTables;
     classTables.carve(dClassTables, J);
     cudaError_t error;
@@ -496,6 +502,18 @@ int construct(sadcs_gpu_context* c, const Batch& b, Io& io, cudaStream_t stream,
     if ((error = cudaMemcpyAsync(meta, h, 4 * (5 * static_cast<size_t>(J) + 1 + b.classTables.size()),
                                  cudaMemcpyHostToDevice, stream)) != cudaSuccess) {
         return failed("tables", error);
+    }
+    if (io.saPieces || io.bwtPieces) {
+        uint32_t* after = h + 5 * J + 1 + b.classTables.size();
+        uint64_t* hp = reinterpret_cast<uint64_t*>(after + ((after - c->hostWords) & 1));
+        for (uint32_t j = 0; j < J; j++) {
+            hp[j] = io.saPieces ? reinterpret_cast<uint64_t>(io.saPieces[j]) : 0;
+            hp[J + j] = io.bwtPieces ? reinterpret_cast<uint64_t>(io.bwtPieces[j]) : 0;
+        }
+        if ((error = cudaMemcpyAsync(dPieces, hp, 16 * static_cast<size_t>(J), cudaMemcpyHostToDevice, stream)) !=
+            cudaSuccess) {
+            return failed("tables", error);
+        }
     }
 
     TextSet texts{};
@@ -612,13 +630,16 @@ int construct(sadcs_gpu_context* c, const Batch& b, Io& io, cudaStream_t stream,
     start = std::chrono::steady_clock::now();
 
     // Merge.
-    uint32_t* sa = io.outSa ? io.outSa : (io.wantSa ? reinterpret_cast<uint32_t*>(slab + L.sa) : nullptr);
-    uint8_t* bwt = io.outBwt ? io.outBwt : (io.wantBwt ? slab + L.bwt : nullptr);
+    uint32_t* const* saPieces = io.saPieces ? reinterpret_cast<uint32_t* const*>(dPieces) : nullptr;
+    uint8_t* const* bwtPieces = io.bwtPieces ? reinterpret_cast<uint8_t* const*>(dPieces + J) : nullptr;
+    uint32_t* sa = saPieces ? nullptr
+                            : (io.outSa ? io.outSa : (io.wantSa ? reinterpret_cast<uint32_t*>(slab + L.sa) : nullptr));
+    uint8_t* bwt = bwtPieces ? nullptr : (io.outBwt ? io.outBwt : (io.wantBwt ? slab + L.bwt : nullptr));
     if ((error = mergeClasses(text, ranks, texts, lists, b.merge, classTables.rowBase, dOutBase, dRowZero,
                               reinterpret_cast<uint32_t*>(slab + L.splitters),
                               reinterpret_cast<MergeRow*>(slab + L.rows), sa, bwt,
                               reinterpret_cast<uint32_t*>(slab + L.mergeCounter), c->hostWords, stream,
-                              c->events[4], c->events[5])) != cudaSuccess) {
+                              c->events[4], c->events[5], saPieces, bwtPieces)) != cudaSuccess) {
         return failed("merge", error);
     }
     cudaEventRecord(c->events[3], stream);

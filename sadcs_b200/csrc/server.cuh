@@ -98,6 +98,8 @@ void serveBatch(sadcs_gpu_server* srv, sadcs_gpu_context& ctx, std::vector<Serve
         io.wantSa = true;
         io.wantBwt = true;
         std::vector<const uint8_t*> pieces;
+        std::vector<uint32_t*> saPieces;
+        std::vector<uint8_t*> bwtPieces;
         if (group.size() == 1) {
             io.hostText = group[0]->text;
             // Page-locked outputs are written by the merge itself (see sadcs_gpu_build_batch).
@@ -108,16 +110,31 @@ void serveBatch(sadcs_gpu_server* srv, sadcs_gpu_context& ctx, std::vector<Serve
             // region (asynchronous from page-locked memory; the driver stages pageable memory).
             for (ServerRequest* r : group) pieces.push_back(r->text);
             io.hostPieces = pieces.data();
+            // When every request's outputs are page-locked, the merge writes each into its own.
+            bool mapped = true;
+            for (ServerRequest* r : group) {
+                uint32_t* s = static_cast<uint32_t*>(mappedHost(r->sa));
+                uint8_t* w = static_cast<uint8_t*>(mappedHost(r->bwt));
+                mapped = mapped && s && w;
+                saPieces.push_back(s);
+                bwtPieces.push_back(w);
+            }
+            if (mapped) {
+                io.saPieces = saPieces.data();
+                io.bwtPieces = bwtPieces.data();
+            }
         }
         status = construct(&ctx, b, io, ctx.stream, stats);
         constructed = nowSeconds();
         if (status == SADCS_OK) {
             uint64_t offset = 0;
             for (ServerRequest* r : group) {
-                if ((!io.outSa && (error = cudaMemcpyAsync(r->sa, io.deviceSa + offset, 4 * r->n,
-                                                           cudaMemcpyDeviceToHost, ctx.stream)) != cudaSuccess) ||
-                    (!io.outBwt && (error = cudaMemcpyAsync(r->bwt, io.deviceBwt + offset, r->n,
-                                                            cudaMemcpyDeviceToHost, ctx.stream)) != cudaSuccess)) {
+                if ((!io.outSa && !io.saPieces &&
+                     (error = cudaMemcpyAsync(r->sa, io.deviceSa + offset, 4 * r->n, cudaMemcpyDeviceToHost,
+                                              ctx.stream)) != cudaSuccess) ||
+                    (!io.outBwt && !io.bwtPieces &&
+                     (error = cudaMemcpyAsync(r->bwt, io.deviceBwt + offset, r->n, cudaMemcpyDeviceToHost,
+                                              ctx.stream)) != cudaSuccess)) {
                     status = failed("download", error);
                     break;
                 }

@@ -260,3 +260,31 @@ def test_page_locked_outputs_written_by_the_device(n):
     finally:
         sa.free_pinned(raw_sa)
         sa.free_pinned(raw_bwt)
+
+
+def test_server_page_locked_outputs_in_batches():
+    """Requests whose outputs are page-locked: the batched merge writes each request's SA and BWT
+    into that request's own buffers; every result equals its text built alone."""
+    texts = W.batch_texts(40, lo=1 << 10, hi=1 << 17, seed=14) + [W.natural_text(1 << 20, seed=15)]
+    lengths = [len(t) for t in texts]
+    raw = sa.allocate_pinned(sum(5 * n + 64 for n in lengths))
+    try:
+        views, at = [], 0
+        for n in lengths:
+            out_sa = raw[at:at + 4 * n].view(np.uint32)
+            at += (4 * n + 15) // 16 * 16
+            out_bwt = raw[at:at + n]
+            at += (n + 15) // 16 * 16
+            out_sa[:] = 0xFFFFFFFF
+            views.append((out_sa, out_bwt))
+        with sa.Server(workers=2, small_limit=1 << 20, batch_bytes=64 << 20, batch_texts=64) as server:
+            tickets = [server.submit(t, sa=v[0], bwt=v[1]) for t, v in zip(texts, views)]
+            batched = 0
+            for k, ticket in enumerate(tickets):
+                s_, b_, p_, _, size = server.wait(ticket)
+                es, eb, ep = _expected(texts[k])
+                assert np.array_equal(s_, es) and np.array_equal(b_, eb) and p_ == ep, f"request {k} differs"
+                batched += size > 1
+            assert batched > 0
+    finally:
+        sa.free_pinned(raw)
