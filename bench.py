@@ -410,7 +410,7 @@ def run_ours(args, world, rank, local) -> None:
     merge_avg = sum(merge_ms) / len(merge_ms)
     merge_gbs = MERGE_BYTES_PER_INPUT_BYTE * n / (merge_avg / 1e3) / 1e9
     pipe_gbs = PIPELINE_BYTES_PER_INPUT_BYTE * n / (ms / 1e3) / 1e9
-    roofline = {"bound": "hbm", "kernel": "mergeTiles<final> (level-0 tile merge writing SA + BWT)",
+    roofline = {"bound": "hbm", "kernel": "mergeTree<final> (last merge level: tiles of the 7 class lists merged in shared memory, writing SA + BWT)",
                 "achieved": round(merge_gbs, 1), "peak": peak, "unit": "GB/s", "frac": round(merge_gbs / peak, 4),
                 "traffic": None, "algorithmic_bytes_per_input_byte": MERGE_BYTES_PER_INPUT_BYTE,
                 "kernel_ms": round(merge_avg, 3), "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"}
