@@ -21,15 +21,19 @@
 namespace sadcs {
 
 #ifndef SADCS_SEGSORT_BLOCKS
-#define SADCS_SEGSORT_BLOCKS 2  // resident blocks per SM the register budget is set for (tuning)
+#define SADCS_SEGSORT_BLOCKS 4  // resident blocks per SM the register budget is set for (tuning)
 #endif
 
-constexpr uint32_t kSegSmall = 2048;                 // largest segment sorted in one block
-constexpr uint32_t kSegChunk = 2048;                 // a block owns the segments starting in such a range
+#ifndef SADCS_SEGSORT_SMALL
+#define SADCS_SEGSORT_SMALL 1024  // largest segment sorted in shared memory (tuning; 1024 with 4 blocks per SM: 1.4 ms less ranking at 256 MiB than 2048 with 2)
+#endif
+
+constexpr uint32_t kSegSmall = SADCS_SEGSORT_SMALL;  // largest segment sorted in one block
+constexpr uint32_t kSegChunk = SADCS_SEGSORT_SMALL;  // a block owns the segments starting in such a range
 constexpr uint32_t kSegCap = kSegChunk + kSegSmall;  // elements a block can hold
 constexpr int kSegThreads = 256;
 constexpr int kSegWarps = kSegThreads / 32;
-constexpr int kSegItems = kSegCap / kSegThreads;     // 16
+constexpr int kSegItems = kSegCap / kSegThreads;     // 8 at the default
 constexpr uint32_t kSegMaxLocal = kSegChunk;         // segments starting in a chunk (each has >= 1 element)
 
 // The segments' big-path tables (host-sized): begin, size and first tile of each big segment.
@@ -95,59 +99,42 @@ __global__ void segCollectBig(const uint32_t* __restrict__ heads, uint32_t segme
     if (k == 0) tileStart[bigCount] = totalTiles;
 }
 
-// hist[(p * big + s) * 256 + digit] for every pass p of big segment s (zeroed by the caller). Runs
-// of equal digits are counted in registers and added to the shared histogram when the digit
-// changes, as in radixHistogram.
-__global__ void __launch_bounds__(256) segHistogram(const uint64_t* __restrict__ keys, ListSegments segs,
-                                                    uint32_t big, int passes, uint32_t* __restrict__ hist) {
-    __shared__ uint32_t h[8][256];
-    for (int i = threadIdx.x; i < 8 * 256; i += blockDim.x) (&h[0][0])[i] = 0;
+// hist[s * 256 + digit] of digit pass `pass` (bits [8 * pass, 8 * pass + 8)) of every big segment s
+// (zeroed by the caller). One histogram per pass, made just before the pass, so that the table is
+// big x 256 words, not passes times that. Runs of equal digits are counted in registers and added
+// to the shared histogram when the digit changes, as in radixHistogram.
+__global__ void __launch_bounds__(256) segHistogram(const uint64_t* __restrict__ keys, ListSegments segs, int pass,
+                                                    uint32_t* __restrict__ hist) {
+    __shared__ uint32_t h[256];
+    h[threadIdx.x] = 0;
     __syncthreads();
     uint32_t segment, firstTile, begin, size;
     segs.locate(blockIdx.x, segment, firstTile, begin, size);
     const uint32_t local = blockIdx.x - firstTile;
     const uint32_t tileEnd = min((local + 1) * kSortTile, size);
-    uint32_t run[8], digit[8];
-#pragma unroll
-    for (int p = 0; p < 8; p++) {
-        run[p] = 0;
-        digit[p] = 0;
-    }
+    uint32_t run = 0, digit = 0;
     for (uint32_t k = local * kSortTile + threadIdx.x; k < tileEnd; k += blockDim.x) {
-        const uint64_t key = keys[begin + k];
-#pragma unroll
-        for (int p = 0; p < 8; p++) {
-            if (p < passes) {
-                const uint32_t d = static_cast<uint32_t>(key >> (8 * p)) & 0xFF;
-                if (d != digit[p]) {
-                    if (run[p]) atomicAdd(&h[p][digit[p]], run[p]);
-                    digit[p] = d;
-                    run[p] = 0;
-                }
-                run[p]++;
-            }
+        const uint32_t d = static_cast<uint32_t>(keys[begin + k] >> (8 * pass)) & 0xFF;
+        if (d != digit) {
+            if (run) atomicAdd(&h[digit], run);
+            digit = d;
+            run = 0;
         }
+        run++;
     }
-#pragma unroll
-    for (int p = 0; p < 8; p++) {
-        if (p < passes && run[p]) atomicAdd(&h[p][digit[p]], run[p]);
-    }
+    if (run) atomicAdd(&h[digit], run);
     __syncthreads();
-    for (int i = threadIdx.x; i < passes * 256; i += blockDim.x) {
-        const int p = i / 256, d = i % 256;
-        if (h[p][d]) atomicAdd(hist + (static_cast<size_t>(p) * big + segment) * 256 + d, h[p][d]);
-    }
+    if (h[threadIdx.x]) atomicAdd(hist + static_cast<size_t>(segment) * 256 + threadIdx.x, h[threadIdx.x]);
 }
 
-// Row r = p * big + s of hist becomes begin[s] + its exclusive prefix. One block per row.
-__global__ void __launch_bounds__(256) segDigitBase(uint32_t* __restrict__ hist, const uint32_t* __restrict__ begin,
-                                                    uint32_t big) {
+// Row s of hist becomes begin[s] + its exclusive prefix. One block per big segment.
+__global__ void __launch_bounds__(256) segDigitBase(uint32_t* __restrict__ hist, const uint32_t* __restrict__ begin) {
     __shared__ uint32_t warpTotals[32];
     uint32_t* row = hist + static_cast<size_t>(blockIdx.x) * 256;
     const uint32_t v = row[threadIdx.x];
     uint32_t total;
     const uint32_t inclusive = blockInclusiveScan<OpSum>(v, warpTotals, total);
-    row[threadIdx.x] = begin[blockIdx.x % big] + inclusive - v;
+    row[threadIdx.x] = begin[blockIdx.x] + inclusive - v;
 }
 
 // Copies the big segments' ranges from one buffer pair to the other.
@@ -324,7 +311,7 @@ constexpr size_t segSortSharedBytes() {
 inline size_t segScratchWords(uint64_t u) {
     const uint64_t big = u / (kSegSmall + 1) + 2;
     const uint64_t tiles = u / kSortTile + big + 2;
-    return static_cast<size_t>(8 * big * 256 + 3 * (big + 1) + tiles * 256 + 256);
+    return static_cast<size_t>(big * 256 + 3 * (big + 1) + tiles * 256 + 256);
 }
 
 struct SegBuffers {
@@ -378,23 +365,23 @@ inline cudaError_t segmentedSort(const uint32_t* grp, uint32_t u, uint64_t* keys
     uint32_t* tileStart = size + big + 1;
     uint32_t* hist = tileStart + big + 1;
     const int passes = (keyBits + 7) / 8;
-    uint32_t* statusWords = hist + static_cast<size_t>(passes) * big * 256;
+    uint32_t* statusWords = hist + static_cast<size_t>(big) * 256;
     const RadixScratch radix = RadixScratch::at(b.radixControl, statusWords);
     SADCS_TRY(launch(segCollectBig, ceilDiv(segments, 256), 256, 0, stream, b.heads, segments, bigFlag, tiles, big,
                      bigTiles, begin, size, tileStart));
     ListSegments segs{tileStart, begin, size, big};
-    SADCS_TRY(cudaMemsetAsync(hist, 0, static_cast<size_t>(passes) * big * 256 * 4, stream));
-    SADCS_TRY(launch(segHistogram, bigTiles, 256, 0, stream, keys, segs, big, passes, hist));
-    SADCS_TRY(launch(segDigitBase, static_cast<uint32_t>(passes) * big, 256, 0, stream, hist, begin, big));
     uint64_t* kIn = keys;
     uint64_t* kOut = keysAlt;
     uint32_t* vIn = vals;
     uint32_t* vOut = valsAlt;
     for (int p = 0; p < passes; p++) {
+        SADCS_TRY(cudaMemsetAsync(hist, 0, static_cast<size_t>(big) * 256 * 4, stream));
+        SADCS_TRY(launch(segHistogram, bigTiles, 256, 0, stream, kIn, segs, p, hist));
+        SADCS_TRY(launch(segDigitBase, big, 256, 0, stream, hist, begin));
         SortLoader<uint64_t> ld{kIn, vIn, 8 * p};
         SortStorer<uint64_t> st{kOut, vOut, u};
         SADCS_TRY((radixOnesweepPass<uint64_t, SortLoader<uint64_t>, SortStorer<uint64_t>, ListSegments>(
-            ld, st, segs, u, bigTiles, hist + static_cast<size_t>(p) * big * 256, radix, stream)));
+            ld, st, segs, u, bigTiles, hist, radix, stream)));
         std::swap(kIn, kOut);
         std::swap(vIn, vOut);
     }
