@@ -80,9 +80,13 @@ __device__ __forceinline__ FinalHead loadHead(const FinalTile<W, kMulti>& s, uin
     return h;
 }
 
-// Suffix a < suffix b, by the difference-cover comparison (merge.cuh: lessRecord): texts by their
-// end, then the first k = tie offset characters (at most the shorter suffix's length), then the
-// sample ranks at a + k and b + k; a suffix that is a prefix of the other is the smaller.
+// Suffix a < suffix b, by the difference-cover comparison (merge.cuh: lessRecord), cheapest test
+// first. The records hold at least the first 31 characters of each suffix. If those differ, the
+// first difference orders the suffixes whatever the cover's tie offset k: compared characters past
+// a single text's end are code 0, the smallest, so the shorter suffix is the smaller there too, as
+// it must be; with several texts the stream continues into the next text, so the words are masked
+// to the shorter suffix. Only when all compared characters agree (hence the first k, k < 32) do the
+// sample ranks at a + k and b + k decide, or the lengths when one suffix ends within k.
 template <int W, bool kMulti>
 __device__ __forceinline__ bool headLess(const FinalTile<W, kMulti>& s, const FinalHead& a, const FinalHead& b,
                                          uint32_t n, uint32_t bits) {
@@ -91,30 +95,37 @@ __device__ __forceinline__ bool headLess(const FinalTile<W, kMulti>& s, const Fi
         n = a.end;
     }
     const uint32_t i = a.pos, j = b.pos;
-    const uint32_t k = tieOffset(a.rot, b.rot);
-    const uint32_t common = min(k, min(n - i, n - j));
-    const uint32_t cbits = common * bits;
-    {
+    if constexpr (kMulti) {
+        const uint32_t lim = min(n - i, n - j) * bits;  // bits of the shorter suffix
         uint64_t x = a.w0, y = b.w0;
-        if (cbits < 64) {
-            const uint64_t mk = cbits ? ~uint64_t(0) << (64 - cbits) : 0;
+        if (lim < 64) {
+            const uint64_t mk = lim ? ~uint64_t(0) << (64 - lim) : 0;
             x &= mk;
             y &= mk;
         }
         if (x != y) return x < y;
-    }
 #pragma unroll
-    for (int w = 1; w < W; w++) {
-        if (cbits <= 64u * w) break;
-        uint64_t x = s.words[w * kMergeCap + a.idx], y = s.words[w * kMergeCap + b.idx];
-        if (cbits < 64u * (w + 1)) {
-            const uint64_t mk = ~uint64_t(0) << (64u * (w + 1) - cbits);
-            x &= mk;
-            y &= mk;
+        for (int w = 1; w < W; w++) {
+            if (lim <= 64u * w) break;
+            x = s.words[w * kMergeCap + a.idx];
+            y = s.words[w * kMergeCap + b.idx];
+            if (lim < 64u * (w + 1)) {
+                const uint64_t mk = ~uint64_t(0) << (64u * (w + 1) - lim);
+                x &= mk;
+                y &= mk;
+            }
+            if (x != y) return x < y;
         }
-        if (x != y) return x < y;
+    } else {
+        if (a.w0 != b.w0) return a.w0 < b.w0;
+#pragma unroll
+        for (int w = 1; w < W; w++) {
+            const uint64_t x = s.words[w * kMergeCap + a.idx], y = s.words[w * kMergeCap + b.idx];
+            if (x != y) return x < y;
+        }
     }
-    if (common < k || i + k == n || j + k == n) return i > j;  // one is a prefix of the other
+    const uint32_t k = tieOffset(a.rot, b.rot);
+    if (k > min(n - i, n - j) || i + k == n || j + k == n) return i > j;  // one is a prefix of the other
     return s.rank[sampleSlot(a.rot, k) * kMergeCap + a.idx] < s.rank[sampleSlot(b.rot, k) * kMergeCap + b.idx];
 }
 
