@@ -33,7 +33,7 @@ constexpr uint32_t kMergeG = 32;
 constexpr uint32_t kMergeR = SADCS_MERGE_R;
 constexpr uint32_t kMergeCap = kMergeG * kMergeR + 6 * (kMergeG - 1) + 1;
 #ifndef SADCS_MERGE_THREADS
-#define SADCS_MERGE_THREADS 256
+#define SADCS_MERGE_THREADS 384
 #endif
 constexpr int kMergeThreads = SADCS_MERGE_THREADS;  // threads per tile (tuning)
 constexpr uint32_t kNoList = 0xFFFFFFFFu;
