@@ -118,7 +118,7 @@ struct ClassLoader {
     __device__ __forceinline__ bool load(uint32_t j, uint32_t, uint32_t k, uint8_t& key, uint32_t& dig) const {
         const uint32_t start = texts.startOf(j), end = texts.endOfText(j);
         const uint32_t p = element(j, k);
-        if (p <= start || p > end || cCover.classOf[(p - 1) % kV] != d) return false;
+        if (p <= start || p > end || classOfResidue((p - 1) % kV) != d) return false;
         dig = charCode(texts, p - 1);  // codes order like the bytes they stand for
         key = static_cast<uint8_t>(dig);
         return true;
@@ -155,7 +155,7 @@ __global__ void __launch_bounds__(256) classHistogram(uint32_t total, TextSet te
         for (int k = 0; k < 8; k++) {
             const uint64_t q = base + k;
             const uint32_t c = static_cast<uint32_t>(chunk >> (64 - (k + 1) * b)) & ((1u << b) - 1);
-            const uint32_t cls = q < end ? cCover.classOf[q % kV] : 0;
+            const uint32_t cls = q < end ? classOfResidue(static_cast<uint32_t>(q % kV)) : 0;
             if (cls) {
                 if (one) {
                     atomicAdd(&h[cls * 256 + c], 1u);

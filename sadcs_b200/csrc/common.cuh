@@ -104,12 +104,27 @@ inline uint64_t packHost(uint64_t p) {
     return (p / kV) * kK + kCoverTables.below[p % kV];
 }
 
+// The cover's residues as 5-bit fields of one word, in increasing order.
+constexpr uint64_t coverResidues() {
+    uint64_t packed = 0;
+    for (int k = 0; k < kK; k++) packed |= static_cast<uint64_t>(kCoverTables.residue[k]) << (5 * k);
+    return packed;
+}
+constexpr uint64_t kCoverResidues = coverResidues();
+
+// Device lookups of the cover by register arithmetic on its mask: a warp indexes them with
+// different residues, which a __constant__ table would serve one address at a time.
 __device__ __forceinline__ uint32_t pack(uint32_t p) {
-    return (p / kV) * kK + cCover.below[p % kV];
+    return (p / kV) * kK + static_cast<uint32_t>(__popc(kCoverMask & ((1u << (p % kV)) - 1)));
 }
 
 __device__ __forceinline__ uint32_t samplePosition(uint32_t t) {
-    return (t / kK) * kV + cCover.residue[t % kK];
+    return (t / kK) * kV + static_cast<uint32_t>((kCoverResidues >> (5 * (t % kK))) & 31);
+}
+
+// Distance from residue r to the next sampled residue: its class.
+__device__ __forceinline__ uint32_t classOfResidue(uint32_t r) {
+    return static_cast<uint32_t>(__ffs(__funnelshift_r(kCoverMask, kCoverMask, r))) - 1;
 }
 
 inline uint64_t sampleSize(uint64_t n) {
