@@ -8,10 +8,12 @@
 //
 // One pass: key every listed suffix by a subkey, sort the list stably by (group id, subkey), split
 // groups where the subkey changes (a new group's id is its old id plus its offset inside the old
-// group, propagated by max-scans), write the ids, and compact away the singletons.
-//   character passes: the 7 characters at p + depth in the top 56 bits and min(remaining, 7) in the
-//     low byte (0 at or past the end), so a suffix that ends inside the window is separated from
-//     every longer one sharing its characters; depth 0, 7, 14, 21, 28 (35 >= 32 characters shared)
+// group, from the last old and new group heads before each element), write the ids, and compact
+// away the singletons (three fused kernels per pass, below).
+//   character passes: the keyChars codes at p + depth (alphabet.cuh: 29 for DNA, 10 for 6-bit text,
+//     7 for bytes) in the top bits and min(remaining, keyChars) in the low tag bits (code 0 at or
+//     past the end), so a suffix that ends inside the window is separated from every longer one
+//     sharing its characters; depth grows by keyChars until it reaches 32
 //   doubling rounds: 1 + the group id at p + h (0 past the end), h the largest multiple of 32 not
 //     above the shared depth, so p + h is again a sample position; depth grows by h each round.
 // Every subkey of a pass is read before any id of that pass is written.
@@ -109,42 +111,162 @@ __global__ void rankGatherGroups(const uint32_t* __restrict__ ranks, const uint3
     if (i < u) grp[i] = lst[i] < m ? ranks[lst[i]] : 0;
 }
 
-// aux1[i] = grp[i] - i at the first element of an old group (>= 0: every listed element before it
-// belongs to a smaller group), else 0; its max-scan is grp - (start of the old group) everywhere.
-__global__ void rankOldHeads(const uint32_t* __restrict__ grp, uint32_t* __restrict__ aux1, uint32_t u) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= u) return;
-    const bool head = i == 0 || grp[i] != grp[i - 1];
-    aux1[i] = head ? grp[i] - i : 0;
+// ---- the refinement after a pass's sort, fused ------------------------------------------------
+//
+// With the list sorted by (group, key): an element starts an old group where its group id changes,
+// a new group where its group id or its key changes; its new id is its old id plus (index of its
+// new group's head - index of its old group's head), because ids are ranks of group heads; it stays
+// listed unless its new group is a singleton. Three kernels over tiles of 4096 elements: per-tile
+// aggregates (last old head, last new head, kept count), their scan, then each tile again with the
+// carries: ids written to the rank array, kept elements compacted into the other list buffer.
+
+constexpr int kRefineThreads = 256;
+constexpr int kRefineItems = 16;
+constexpr uint32_t kRefineTile = kRefineThreads * kRefineItems;
+
+// Bit k of old / next: element base + k starts an old / a new group (next has bit 16 for base + 16);
+// keep: element base + k stays listed. Elements at or past u have no bits. g: their group ids.
+__device__ __forceinline__ void refineFlags(const uint32_t* __restrict__ grp, const uint64_t* __restrict__ key,
+                                            uint32_t u, uint32_t base, uint32_t g[kRefineItems], uint32_t& old,
+                                            uint32_t& next, uint32_t& keep) {
+    uint32_t prevG = base > 0 && base - 1 < u ? grp[base - 1] : 0xFFFFFFFFu;
+    uint64_t prevK = base > 0 && base - 1 < u ? key[base - 1] : 0;
+    old = 0;
+    next = 0;
+#pragma unroll
+    for (int k = 0; k <= kRefineItems; k++) {
+        const uint32_t e = base + k;
+        if (e >= u) break;
+        const uint32_t ge = grp[e];
+        const uint64_t ke = key[e];
+        const bool startOld = e == 0 || ge != prevG;
+        if (k < kRefineItems) {
+            g[k] = ge;
+            if (startOld) old |= 1u << k;
+        }
+        if (startOld || ke != prevK) next |= 1u << k;
+        prevG = ge;
+        prevK = ke;
+    }
+    keep = 0;
+#pragma unroll
+    for (int k = 0; k < kRefineItems; k++) {
+        const uint32_t e = base + k;
+        if (e >= u) break;
+        const bool single = ((next >> k) & 1) && (e + 1 == u || ((next >> (k + 1)) & 1));
+        if (!single) keep |= 1u << k;
+    }
 }
 
-__device__ __forceinline__ bool newHead(const uint32_t* grp, const uint64_t* key, uint32_t i) {
-    return i == 0 || grp[i] != grp[i - 1] || key[i] != key[i - 1];
+// agg[tile], agg[tiles + tile], agg[2 * tiles + tile] = last old head, last new head, kept count.
+__global__ void __launch_bounds__(kRefineThreads) rankRefineReduce(const uint32_t* __restrict__ grp,
+                                                                   const uint64_t* __restrict__ key, uint32_t u,
+                                                                   uint32_t tiles, uint32_t* __restrict__ agg) {
+    __shared__ uint32_t warpOld[kRefineThreads / 32], warpNew[kRefineThreads / 32], warpKept[kRefineThreads / 32];
+    const uint32_t base = blockIdx.x * kRefineTile + threadIdx.x * kRefineItems;
+    uint32_t g[kRefineItems], old, next, keep;
+    refineFlags(grp, key, u, base, g, old, next, keep);
+    const uint32_t mine = next & 0xFFFFu;
+    uint32_t lastOld = old ? base + 31 - __clz(old) : 0;
+    uint32_t lastNew = mine ? base + 31 - __clz(mine) : 0;
+    uint32_t kept = __popc(keep);
+    lastOld = __reduce_max_sync(0xffffffffu, lastOld);
+    lastNew = __reduce_max_sync(0xffffffffu, lastNew);
+    kept = __reduce_add_sync(0xffffffffu, kept);
+    const uint32_t warp = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) {
+        warpOld[warp] = lastOld;
+        warpNew[warp] = lastNew;
+        warpKept[warp] = kept;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t o = 0, w = 0, c = 0;
+        for (int i = 0; i < kRefineThreads / 32; i++) {
+            o = max(o, warpOld[i]);
+            w = max(w, warpNew[i]);
+            c += warpKept[i];
+        }
+        agg[blockIdx.x] = o;
+        agg[tiles + blockIdx.x] = w;
+        agg[2 * tiles + blockIdx.x] = c;
+    }
 }
 
-// aux2[i] = i + delta at the first element of a new group, else 0; its max-scan is every id.
-__global__ void rankNewHeads(const uint32_t* __restrict__ grp, const uint64_t* __restrict__ key,
-                             const uint32_t* __restrict__ delta, uint32_t* __restrict__ aux2, uint32_t u) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= u) return;
-    aux2[i] = newHead(grp, key, i) ? i + delta[i] : 0;
+// The aggregates become exclusive prefixes (max, max, sum) over the tiles; total = all kept.
+__global__ void __launch_bounds__(256) rankRefineScan(uint32_t* __restrict__ agg, uint32_t tiles,
+                                                      uint32_t* __restrict__ total) {
+    __shared__ uint32_t warpTotals[32];
+    uint32_t carryOld = 0, carryNew = 0, carryKept = 0;
+    for (uint32_t base = 0; base < tiles; base += blockDim.x) {
+        const uint32_t t = base + threadIdx.x;
+        const uint32_t o = t < tiles ? agg[t] : 0;
+        const uint32_t w = t < tiles ? agg[tiles + t] : 0;
+        const uint32_t c = t < tiles ? agg[2 * tiles + t] : 0;
+        uint32_t chunkOld, chunkNew, chunkKept;
+        const uint32_t io = blockInclusiveScan<OpMax>(o, warpTotals, chunkOld);
+        const uint32_t iw = blockInclusiveScan<OpMax>(w, warpTotals, chunkNew);
+        const uint32_t ic = blockInclusiveScan<OpSum>(c, warpTotals, chunkKept);
+        // exclusive prefixes: the inclusive one of the thread before (a shuffle within the warp, the
+        // warp before through a second scan would cost more than recomputing from inclusive - own)
+        if (t < tiles) {
+            agg[2 * tiles + t] = carryKept + ic - c;
+        }
+        __syncthreads();
+        // max is not invertible: publish inclusive values, read the neighbour's
+        __shared__ uint32_t incOld[256], incNew[256];
+        incOld[threadIdx.x] = io;
+        incNew[threadIdx.x] = iw;
+        __syncthreads();
+        if (t < tiles) {
+            agg[t] = max(carryOld, threadIdx.x ? incOld[threadIdx.x - 1] : 0u);
+            agg[tiles + t] = max(carryNew, threadIdx.x ? incNew[threadIdx.x - 1] : 0u);
+        }
+        carryOld = max(carryOld, chunkOld);
+        carryNew = max(carryNew, chunkNew);
+        carryKept += chunkKept;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *total = carryKept;
 }
 
-// Writes the ids; flags[i] = 1 for elements still in a group of two or more.
-__global__ void rankStore(const uint32_t* __restrict__ grp, const uint64_t* __restrict__ key,
-                          const uint32_t* __restrict__ ids, const uint32_t* __restrict__ lst,
-                          uint32_t* __restrict__ ranks, uint32_t* __restrict__ flags, uint32_t u, uint32_t m) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= u) return;
-    if (lst[i] < m) ranks[lst[i]] = ids[i];
-    const bool single = newHead(grp, key, i) && (i + 1 == u || newHead(grp, key, i + 1));
-    flags[i] = single ? 0 : 1;
-}
-
-__global__ void rankCompact(const uint32_t* __restrict__ lst, const uint32_t* __restrict__ flags,
-                            const uint32_t* __restrict__ slots, uint32_t* __restrict__ out, uint32_t u) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < u && flags[i]) out[slots[i]] = lst[i];
+// Each tile again with its carries: ids into the rank array, kept elements compacted into out.
+__global__ void __launch_bounds__(kRefineThreads) rankRefineApply(const uint32_t* __restrict__ grp,
+                                                                  const uint64_t* __restrict__ key,
+                                                                  const uint32_t* __restrict__ lst, uint32_t u,
+                                                                  uint32_t slots, uint32_t tiles,
+                                                                  const uint32_t* __restrict__ agg,
+                                                                  uint32_t* __restrict__ ranks,
+                                                                  uint32_t* __restrict__ out) {
+    __shared__ uint32_t warpTotals[32];
+    __shared__ uint32_t incOld[kRefineThreads], incNew[kRefineThreads];
+    const uint32_t base = blockIdx.x * kRefineTile + threadIdx.x * kRefineItems;
+    uint32_t g[kRefineItems], old, next, keep;
+    refineFlags(grp, key, u, base, g, old, next, keep);
+    const uint32_t mine = next & 0xFFFFu;
+    const uint32_t lastOld = old ? base + 31 - __clz(old) : 0;
+    const uint32_t lastNew = mine ? base + 31 - __clz(mine) : 0;
+    const uint32_t kept = __popc(keep);
+    uint32_t totalOld, totalNew, totalKept;
+    const uint32_t io = blockInclusiveScan<OpMax>(lastOld, warpTotals, totalOld);
+    const uint32_t iw = blockInclusiveScan<OpMax>(lastNew, warpTotals, totalNew);
+    const uint32_t ic = blockInclusiveScan<OpSum>(kept, warpTotals, totalKept);
+    incOld[threadIdx.x] = io;
+    incNew[threadIdx.x] = iw;
+    __syncthreads();
+    uint32_t runOld = max(agg[blockIdx.x], threadIdx.x ? incOld[threadIdx.x - 1] : 0u);
+    uint32_t runNew = max(agg[tiles + blockIdx.x], threadIdx.x ? incNew[threadIdx.x - 1] : 0u);
+    uint32_t at = agg[2 * tiles + blockIdx.x] + ic - kept;
+#pragma unroll
+    for (int k = 0; k < kRefineItems; k++) {
+        const uint32_t e = base + k;
+        if (e >= u) break;
+        if ((old >> k) & 1) runOld = e;
+        if ((next >> k) & 1) runNew = e;
+        const uint32_t item = lst[e];
+        if (item < slots) ranks[item] = g[k] + (runNew - runOld);
+        if ((keep >> k) & 1) out[at++] = item;
+    }
 }
 
 inline uint32_t blocks256(uint64_t count) {
@@ -216,13 +338,11 @@ inline cudaError_t rankSample(const uint8_t* text, const TextSet& texts, uint32_
                           b.counter + 4, b.scanScratch};
             SADCS_TRY(segmentedSort(b.grp, u, key, lst, keyAlt, lstAlt, keyBits, sb, hostCounter + 8, stream));
         }
-        SADCS_TRY(launch(rankOldHeads, blocks256(u), 256, 0, stream, b.grp, b.aux1, u));
-        SADCS_TRY((deviceScan<OpMax, true>(b.aux1, b.aux1, u, b.scanScratch, nullptr, stream)));
-        SADCS_TRY(launch(rankNewHeads, blocks256(u), 256, 0, stream, b.grp, key, b.aux1, b.aux2, u));
-        SADCS_TRY((deviceScan<OpMax, true>(b.aux2, b.aux2, u, b.scanScratch, nullptr, stream)));
-        SADCS_TRY(launch(rankStore, blocks256(u), 256, 0, stream, b.grp, key, b.aux2, lst, ranks, b.aux1, u, slots));
-        SADCS_TRY((deviceScan<OpSum, false>(b.aux1, b.aux2, u, b.scanScratch, b.counter, stream)));
-        SADCS_TRY(launch(rankCompact, blocks256(u), 256, 0, stream, lst, b.aux1, b.aux2, lstAlt, u));
+        const uint32_t refineTiles = ceilDiv(u, kRefineTile);
+        SADCS_TRY(launch(rankRefineReduce, refineTiles, kRefineThreads, 0, stream, b.grp, key, u, refineTiles, b.aux1));
+        SADCS_TRY(launch(rankRefineScan, 1, 256, 0, stream, b.aux1, refineTiles, b.counter));
+        SADCS_TRY(launch(rankRefineApply, refineTiles, kRefineThreads, 0, stream, b.grp, key, lst, u, slots, refineTiles,
+                         b.aux1, ranks, lstAlt));
         SADCS_TRY(cudaMemcpyAsync(hostCounter, b.counter, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
         SADCS_TRY(cudaMemcpyAsync(hostCounter + 1, error, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
         SADCS_TRY(cudaStreamSynchronize(stream));
