@@ -2,11 +2,11 @@
 // the last level writes the suffix array and the BWT, an upper level the rows of the level below.
 //
 // A tile's window set (at most kMergeCap records, merge.cuh) is held as arrays of fields, not as
-// records, so the 32 threads of a warp reading one field of 32 records hit 32 different banks:
+// records, so the 32 threads of a warp reading one field of 32 records hit 32 different banks (the
+// sample ranks stay in global memory: only comparisons whose first 31 characters agree read them):
 //   words[W][cap]  the code stream from the suffix's first character, W = ceil(31 * bits / 64)
 //                  64-bit words: every comparison reads k < 32 characters (k = the cover's tie
 //                  offset), so no comparison reads global memory
-//   rank[7][cap]   the 7 sample ranks of [p, p + 32)
 //   pos[cap]       p; end[cap] the end of p's text (several texts only)
 //   prev[cap]      the code of the character before p (the BWT byte)
 //   idxA, idxB     u16 orders of the records
@@ -42,20 +42,20 @@ __host__ __device__ constexpr int finalWords(uint32_t bits) {
 
 template <int W, bool kMulti>
 struct FinalTile {
-    static constexpr size_t kPerRecord = 8 * W + 4 * kK + 4 + (kMulti ? 4 : 0) + 2 + 2 + 1;
+    static constexpr size_t kPerRecord = 8 * W + 4 + (kMulti ? 4 : 0) + 2 + 2 + 1;
     static constexpr size_t sharedBytes() { return kMergeCap * kPerRecord + 64; }
     uint64_t* words;
-    uint32_t* rank;
     uint32_t* pos;
     uint32_t* end;
     uint16_t* idxA;
     uint16_t* idxB;
     uint8_t* prev;
-    __device__ __forceinline__ void carve(unsigned char* smem) {
+    const uint32_t* ranks;  // the sample ranks in global memory: read only when 31 characters agree
+    __device__ __forceinline__ void carve(unsigned char* smem, const uint32_t* sampleRanks) {
         words = reinterpret_cast<uint64_t*>(smem);
-        rank = reinterpret_cast<uint32_t*>(words + W * kMergeCap);
-        pos = rank + kK * kMergeCap;
+        pos = reinterpret_cast<uint32_t*>(words + W * kMergeCap);
         end = pos + kMergeCap;
+        ranks = sampleRanks;
         idxA = reinterpret_cast<uint16_t*>(end + (kMulti ? kMergeCap : 0));
         idxB = idxA + kMergeCap;
         prev = reinterpret_cast<uint8_t*>(idxB + kMergeCap);
@@ -126,7 +126,8 @@ __device__ __forceinline__ bool headLess(const FinalTile<W, kMulti>& s, const Fi
     }
     const uint32_t k = tieOffset(a.rot, b.rot);
     if (k > min(n - i, n - j) || i + k == n || j + k == n) return i > j;  // one is a prefix of the other
-    return s.rank[sampleSlot(a.rot, k) * kMergeCap + a.idx] < s.rank[sampleSlot(b.rot, k) * kMergeCap + b.idx];
+    // rare (2-3% of the comparisons on natural and DNA-like text): the ranks come from global memory
+    return __ldg(s.ranks + pack(i + k)) < __ldg(s.ranks + pack(j + k));
 }
 
 // One tree level: the merges m (A = [mb[3m], mb[3m + 1]), B = [mb[3m + 1], mb[3m + 2]) of src,
@@ -180,7 +181,7 @@ template <int W, bool kMulti, bool kFinal>
 __global__ void __launch_bounds__(kMergeThreads) mergeTree(MergeArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     FinalTile<W, kMulti> s;
-    s.carve(smem);
+    s.carve(smem, a.ranks);
     __shared__ MergeTileInfo t;
     __shared__ uint32_t sLo, sHi;
     __shared__ uint32_t bounds[3 * 7];  // the tree's merges: 4 + 2 + 1 triples of window offsets
@@ -237,9 +238,6 @@ __global__ void __launch_bounds__(kMergeThreads) mergeTree(MergeArgs a) {
             const uint64_t* src = a.texts.packed + ((static_cast<uint64_t>(q) * bits) >> 6);
 #pragma unroll
             for (int w = 0; w < W; w++) cpAsync8(&s.words[w * kMergeCap + e], src + w);
-            const uint32_t* rk = a.ranks + pack(q);
-#pragma unroll
-            for (int r = 0; r < kK; r++) cpAsync4(&s.rank[r * kMergeCap + e], rk + r);
         }
     }
 #pragma unroll
