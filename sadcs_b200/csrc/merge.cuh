@@ -25,10 +25,10 @@
 namespace sadcs {
 
 constexpr uint32_t kMergeG = 32;
-// Rows every R splitters; tiles of at most G * R + 6 * (G - 1) + 1 records (1019 at R = 26). R sets the
+// Rows every R splitters; tiles of at most G * R + 6 * (G - 1) + 1 records (1467 at R = 40). R sets the
 // tile's shared memory and so the blocks per SM; the build may override it (tuning).
 #ifndef SADCS_MERGE_R
-#define SADCS_MERGE_R 26
+#define SADCS_MERGE_R 40
 #endif
 constexpr uint32_t kMergeR = SADCS_MERGE_R;
 constexpr uint32_t kMergeCap = kMergeG * kMergeR + 6 * (kMergeG - 1) + 1;
