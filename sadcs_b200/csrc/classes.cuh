@@ -85,6 +85,12 @@ inline size_t classScratchWords(uint64_t totalLength, uint32_t texts) {
     return static_cast<size_t>(kClasses) * texts * 256 + 8 * 256 + 64 + static_cast<size_t>(tiles) * 256 + 64;
 }
 
+// 64-bit words of one chain buffer: the largest of classes 1 to kClasses - 2 (the last class stores
+// no chains), bounded here by every class's own bound.
+inline size_t classChainWords(uint64_t live) {
+    return static_cast<size_t>(live) + 64;
+}
+
 inline uint32_t* classRadixScratch(uint32_t* scratch, uint32_t texts) {
     return scratch + static_cast<size_t>(kClasses) * texts * 256;
 }
@@ -104,33 +110,58 @@ __global__ void classScatterSample(const uint32_t* __restrict__ ranks, uint32_t 
     if (r < live) list[r] = p;
 }
 
+// Codes of the 8 characters before p: byte i holds the code of T[p - 1 - i] (0 before position 0),
+// from one 64-bit window of the code stream (b <= 8, so 8 codes fit in it).
+__device__ __forceinline__ uint64_t codesBefore(const TextSet& texts, uint32_t p) {
+    const uint32_t b = texts.bits;
+    const uint32_t first = p >= 8 ? p - 8 : 0;
+    const uint64_t window = streamBits(texts.packed, static_cast<uint64_t>(first) * b);
+    const uint64_t mask = (uint64_t(1) << b) - 1;
+    uint64_t chain = 0;
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        const int at = static_cast<int>(p - first) - 1 - i;  // T[p - 1 - i] is character `at` of the window
+        if (at >= 0) chain |= ((window >> (64 - (at + 1) * b)) & mask) << (8 * i);
+    }
+    return chain;
+}
+
 // Element k of text j's class d - 1 with the text's end prepended; keeps p - 1 if it is in class d
-// and in the text, keyed by T[p - 1].
+// and in the text, keyed by the code of T[p - 1]. The sort key is the element's chain: the codes of
+// the characters before it, byte 0 first. Pass 1 reads the chains of the sample positions from the
+// code stream (one window each); later passes read the chains the pass before stored in list order,
+// so only pass 1 reads the text at random positions. A text's end reads its own chain every pass.
 struct ClassLoader {
     const uint32_t* __restrict__ lists;       // global lists
     const uint32_t* __restrict__ prevOffset;  // rowBase row of class d - 1: text j's slice offset
-    const uint8_t* __restrict__ text;
+    const uint64_t* __restrict__ chains;      // chains of class d - 1 by index from prevStart (d >= 2)
+    uint32_t prevStart;                       // first slot of class d - 1 in the global lists
     TextSet texts;
     uint32_t d;
     __device__ __forceinline__ uint32_t element(uint32_t j, uint32_t k) const {
         return k == 0 ? texts.endOfText(j) : lists[__ldg(prevOffset + j) + k - 1];
     }
-    __device__ __forceinline__ bool load(uint32_t j, uint32_t, uint32_t k, uint8_t& key, uint32_t& dig) const {
+    __device__ __forceinline__ bool load(uint32_t j, uint32_t, uint32_t k, uint64_t& key, uint32_t& dig) const {
         const uint32_t start = texts.startOf(j), end = texts.endOfText(j);
         const uint32_t p = element(j, k);
         if (p <= start || p > end || classOfResidue((p - 1) % kV) != d) return false;
-        dig = charCode(texts, p - 1);  // codes order like the bytes they stand for
-        key = static_cast<uint8_t>(dig);
+        key = k == 0 || d == 1 ? codesBefore(texts, p) : chains[__ldg(prevOffset + j) - prevStart + k - 1];
+        dig = static_cast<uint32_t>(key & 0xFF);  // codes order like the bytes they stand for
         return true;
     }
     __device__ __forceinline__ uint32_t value(uint32_t j, uint32_t, uint32_t k) const { return element(j, k) - 1; }
 };
 
+// Writes class d's positions, and (unless chains is null: the last class) the chains of its
+// elements: an element p - 1 has p's chain less its first character.
 struct ClassStorer {
-    static constexpr bool kKeys = false;
+    static constexpr bool kKeys = true;
     uint32_t* __restrict__ lists;
-    uint32_t lo, hi;  // class d's slots in the global lists
-    __device__ __forceinline__ void storeKey(uint32_t, uint32_t, uint8_t) const {}
+    uint64_t* __restrict__ chains;  // by index from lo
+    uint32_t lo, hi;                // class d's slots in the global lists
+    __device__ __forceinline__ void storeKey(uint32_t, uint32_t pos, uint64_t chain) const {
+        if (chains && pos >= lo && pos < hi) chains[pos - lo] = chain >> 8;
+    }
     __device__ __forceinline__ void storeValue(uint32_t, uint32_t pos, uint32_t v) const {
         if (pos >= lo && pos < hi) lists[pos] = v;  // always, unless a look-back timed out
     }
@@ -186,9 +217,10 @@ __global__ void __launch_bounds__(256) classDigitBase(uint32_t* __restrict__ his
 // Fills lists (laid out by plan.start, text-major inside each class) from the sample ranks.
 // tables: the ClassTables block on the device; scratch: classScratchWords(total, J) words.
 // total: bytes of the concatenation (text buffer) scanned by the histogram.
-inline cudaError_t sortClasses(const uint8_t* text, uint32_t total, const TextSet& texts, const uint32_t* ranks,
-                               uint32_t slots, const ClassPlan& plan, const ClassTables& tables, uint32_t* lists,
-                               uint32_t* scratch, cudaStream_t stream) {
+// chains: two buffers of classChainWords(plan) 64-bit words each.
+inline cudaError_t sortClasses(uint32_t total, const TextSet& texts, const uint32_t* ranks, uint32_t slots,
+                               const ClassPlan& plan, const ClassTables& tables, uint32_t* lists, uint32_t* scratch,
+                               uint64_t* const chains[2], cudaStream_t stream) {
     const uint32_t J = tables.texts;
     const uint32_t live = plan.start[1];
     if (live > 0) {
@@ -203,11 +235,12 @@ inline cudaError_t sortClasses(const uint8_t* text, uint32_t total, const TextSe
     SADCS_TRY(launch(classDigitBase, kClasses * J, 256, 0, stream, hist, tables.rowBase));
     for (int d = 1; d < kClasses; d++) {
         if (plan.start[d + 1] == plan.start[d]) continue;
-        ClassLoader ld{lists, tables.rowBase + static_cast<size_t>(d - 1) * J, text, texts, static_cast<uint32_t>(d)};
-        ClassStorer st{lists, plan.start[d], plan.start[d + 1]};
+        ClassLoader ld{lists, tables.rowBase + static_cast<size_t>(d - 1) * J, chains[d & 1], plan.start[d - 1], texts,
+                       static_cast<uint32_t>(d)};
+        ClassStorer st{lists, d + 1 < kClasses ? chains[(d + 1) & 1] : nullptr, plan.start[d], plan.start[d + 1]};
         ManySegments segs{tables.tileStart + static_cast<size_t>(d) * (J + 1),
                           tables.elementStart + static_cast<size_t>(d) * (J + 1), J};
-        SADCS_TRY((radixOnesweepPass<uint8_t, ClassLoader, ClassStorer, ManySegments>(
+        SADCS_TRY((radixOnesweepPass<uint64_t, ClassLoader, ClassStorer, ManySegments>(
             ld, st, segs, plan.inputs[d], plan.tiles[d], hist + static_cast<size_t>(d) * J * 256, radix, stream)));
     }
     return cudaSuccess;

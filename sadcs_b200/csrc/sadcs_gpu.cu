@@ -123,7 +123,8 @@ struct Layout {
     size_t segScratch = 0;
     size_t counter = 0;
     // class + merge region (overlaps the ranking region)
-    size_t lists = 0, classScratch = 0, splitters = 0, rows = 0, sa = 0, bwt = 0, mergeCounter = 0;
+    size_t lists = 0, classScratch = 0, chain0 = 0, chain1 = 0, splitters = 0, rows = 0, sa = 0, bwt = 0,
+           mergeCounter = 0;
     size_t rankingEnd = 0, classEnd = 0, mergeEnd = 0, peak = 0;
 };
 
@@ -193,6 +194,8 @@ Layout planLayout(const Extent& x, bool internalSa, bool internalBwt) {
     at = persistent;
     L.lists = take(4 * x.outputs);
     L.classScratch = take(4 * classScratchWords(x.span, x.count));
+    L.chain0 = take(8 * classChainWords(x.live));
+    L.chain1 = take(8 * classChainWords(x.live));
     L.classEnd = at;
     at = L.classScratch;  // the merge reuses the class scratch
     L.splitters = take(4 * x.splitterWords);
@@ -614,8 +617,9 @@ int construct(sadcs_gpu_context* c, const Batch& b, Io& io, cudaStream_t stream,
     // Class lists.
     uint32_t* lists = reinterpret_cast<uint32_t*>(slab + L.lists);
     uint32_t* classScratch = reinterpret_cast<uint32_t*>(slab + L.classScratch);
-    if ((error = sortClasses(text, J == 1 ? b.end[0] : b.end[J - 1], texts, ranks, static_cast<uint32_t>(b.slots),
-                             b.classes, classTables, lists, classScratch, stream)) != cudaSuccess) {
+    uint64_t* const chains[2] = {reinterpret_cast<uint64_t*>(slab + L.chain0), reinterpret_cast<uint64_t*>(slab + L.chain1)};
+    if ((error = sortClasses(J == 1 ? b.end[0] : b.end[J - 1], texts, ranks, static_cast<uint32_t>(b.slots), b.classes,
+                             classTables, lists, classScratch, chains, stream)) != cudaSuccess) {
         return failed("class sorts", error);
     }
     cudaEventRecord(c->events[2], stream);
