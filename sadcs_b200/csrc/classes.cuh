@@ -144,8 +144,12 @@ struct ClassLoader {
     __device__ __forceinline__ bool load(uint32_t j, uint32_t, uint32_t k, uint64_t& key, uint32_t& dig) const {
         const uint32_t start = texts.startOf(j), end = texts.endOfText(j);
         const uint32_t p = element(j, k);
+        // A stored chain is read for every element, kept or not (the reads are sequential), so that
+        // it is in flight together with the position instead of waiting for the filter.
+        const bool stored = k > 0 && d > 1;
+        const uint64_t chain = stored ? chains[__ldg(prevOffset + j) - prevStart + k - 1] : 0;
         if (p <= start || p > end || classOfResidue((p - 1) % kV) != d) return false;
-        key = k == 0 || d == 1 ? codesBefore(texts, p) : chains[__ldg(prevOffset + j) - prevStart + k - 1];
+        key = stored ? chain : codesBefore(texts, p);
         dig = static_cast<uint32_t>(key & 0xFF);  // codes order like the bytes they stand for
         return true;
     }
