@@ -99,16 +99,22 @@ inline uint32_t* classErrorWord(uint32_t* scratch, uint32_t texts) {
     return radixErrorWord(classRadixScratch(scratch, texts));
 }
 
-// Class 0: the live sample positions in rank order.
-__global__ void classScatterSample(const uint32_t* __restrict__ ranks, uint32_t slots, uint32_t live, TextSet texts,
-                                   uint32_t* __restrict__ list) {
+// Class 0: the live sample positions in rank order, the ranks in [lo, hi) of them. The writes land
+// at random places of the list, so the caller covers the ranks in slices whose part of the list
+// stays in L2 (a 4-byte write to a line that is not there costs a DRAM read and write of its sector).
+__global__ void classScatterSample(const uint32_t* __restrict__ ranks, uint32_t slots, uint32_t lo, uint32_t hi,
+                                   TextSet texts, uint32_t* __restrict__ list) {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= slots) return;
+    const uint32_t r = __ldcs(ranks + t);  // streamed: evicted first, so the list's slice stays
+    if (r < lo || r >= hi) return;
     const uint32_t p = samplePosition(t);
     if (p >= texts.endOf(p)) return;  // past the end, or between texts
-    const uint32_t r = ranks[t];
-    if (r < live) list[r] = p;
+    list[r] = p;
 }
+
+// Ranks per slice of classScatterSample: 12M ranks = 48 MB of list.
+constexpr uint32_t kScatterSlice = 12u << 20;
 
 // Codes of the 8 characters before p: byte i holds the code of T[p - 1 - i] (0 before position 0),
 // from one 64-bit window of the code stream (b <= 8, so 8 codes fit in it).
@@ -227,8 +233,9 @@ inline cudaError_t sortClasses(uint32_t total, const TextSet& texts, const uint3
                                uint64_t* const chains[2], cudaStream_t stream) {
     const uint32_t J = tables.texts;
     const uint32_t live = plan.start[1];
-    if (live > 0) {
-        SADCS_TRY(launch(classScatterSample, (slots + 255) / 256, 256, 0, stream, ranks, slots, live, texts, lists));
+    for (uint32_t lo = 0; lo < live; lo += kScatterSlice) {
+        const uint32_t hi = live - lo > kScatterSlice ? lo + kScatterSlice : live;
+        SADCS_TRY(launch(classScatterSample, (slots + 255) / 256, 256, 0, stream, ranks, slots, lo, hi, texts, lists));
     }
     uint32_t* hist = scratch;  // [kClasses][J][256]
     const RadixScratch radix(classRadixScratch(scratch, J), 0);

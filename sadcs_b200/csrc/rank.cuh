@@ -118,7 +118,11 @@ __global__ void rankGatherGroups(const uint32_t* __restrict__ ranks, const uint3
 // new group's head - index of its old group's head), because ids are ranks of group heads; it stays
 // listed unless its new group is a singleton. Three kernels over tiles of 4096 elements: per-tile
 // aggregates (last old head, last new head, kept count), their scan, then each tile again with the
-// carries: ids written to the rank array, kept elements compacted into the other list buffer.
+// carries: kept elements compacted into the other list buffer with their ids (the next pass's
+// groups, in list order), and ids written to the rank array for the elements whose id is final
+// (singletons) or, when writeAll is set (before and during the doubling rounds, whose keys read the
+// ranks of other samples), for every element. The rank array is indexed by sample position, so
+// each write lands at a random place: the character passes write each sample's rank once.
 
 constexpr int kRefineThreads = 256;
 constexpr int kRefineItems = 16;
@@ -237,7 +241,8 @@ __global__ void __launch_bounds__(kRefineThreads) rankRefineApply(const uint32_t
                                                                   uint32_t slots, uint32_t tiles,
                                                                   const uint32_t* __restrict__ agg,
                                                                   uint32_t* __restrict__ ranks,
-                                                                  uint32_t* __restrict__ out) {
+                                                                  uint32_t* __restrict__ out,
+                                                                  uint32_t* __restrict__ grpOut, uint32_t writeAll) {
     __shared__ uint32_t warpTotals[32];
     __shared__ uint32_t incOld[kRefineThreads], incNew[kRefineThreads];
     const uint32_t base = blockIdx.x * kRefineTile + threadIdx.x * kRefineItems;
@@ -264,8 +269,13 @@ __global__ void __launch_bounds__(kRefineThreads) rankRefineApply(const uint32_t
         if ((old >> k) & 1) runOld = e;
         if ((next >> k) & 1) runNew = e;
         const uint32_t item = lst[e];
-        if (item < slots) ranks[item] = g[k] + (runNew - runOld);
-        if ((keep >> k) & 1) out[at++] = item;
+        const uint32_t id = g[k] + (runNew - runOld);
+        const bool kept = (keep >> k) & 1;
+        if (item < slots && (!kept || writeAll)) ranks[item] = id;
+        if (kept) {
+            grpOut[at] = id;
+            out[at++] = item;
+        }
     }
 }
 
@@ -330,19 +340,26 @@ inline cudaError_t rankSample(const uint8_t* text, const TextSet& texts, uint32_
         if (first) {
             // Everything in one group: one global sort by subkey.
             SADCS_TRY(radixSortPairs<uint64_t>(key, keyAlt, lst, lstAlt, u, 0, keyBits, b.scratch, stream));
-            SADCS_TRY(launch(rankGatherGroups, blocks256(u), 256, 0, stream, ranks, lst, b.grp, u, slots));
+            SADCS_TRY(cudaMemsetAsync(b.grp, 0, static_cast<size_t>(u) * 4, stream));
         } else {
-            // The list holds whole groups in id order: sort inside each group only.
-            SADCS_TRY(launch(rankGatherGroups, blocks256(u), 256, 0, stream, ranks, lst, b.grp, u, slots));
+            // The list holds whole groups in id order: sort inside each group only. Group ids come
+            // with the list from the pass before; the first pass of several texts reads the texts'
+            // first ranks.
+            if (depth == 0) {
+                SADCS_TRY(launch(rankGatherGroups, blocks256(u), 256, 0, stream, ranks, lst, b.grp, u, slots));
+            }
             SegBuffers sb{error - 1, b.aux1, b.aux2, reinterpret_cast<uint32_t*>(keyAlt), b.segScratch,
                           b.counter + 4, b.scanScratch};
             SADCS_TRY(segmentedSort(b.grp, u, key, lst, keyAlt, lstAlt, keyBits, sb, hostCounter + 8, stream));
         }
+        // The next pass reads ranks of other samples when it is a doubling round.
+        const bool writeAll = doubling || depth + texts.keyChars >= kV;
         const uint32_t refineTiles = ceilDiv(u, kRefineTile);
         SADCS_TRY(launch(rankRefineReduce, refineTiles, kRefineThreads, 0, stream, b.grp, key, u, refineTiles, b.aux1));
         SADCS_TRY(launch(rankRefineScan, 1, 256, 0, stream, b.aux1, refineTiles, b.counter));
         SADCS_TRY(launch(rankRefineApply, refineTiles, kRefineThreads, 0, stream, b.grp, key, lst, u, slots, refineTiles,
-                         b.aux1, ranks, lstAlt));
+                         b.aux1, ranks, lstAlt, b.aux2, writeAll ? 1u : 0u));
+        std::swap(b.grp, b.aux2);  // the kept elements' ids are the next pass's groups
         SADCS_TRY(cudaMemcpyAsync(hostCounter, b.counter, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
         SADCS_TRY(cudaMemcpyAsync(hostCounter + 1, error, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
         SADCS_TRY(cudaStreamSynchronize(stream));

@@ -182,7 +182,7 @@ Layout planLayout(const Extent& x, bool internalSa, bool internalBwt) {
     L.lst1 = take(4 * m);
     L.key0 = take(8 * m);
     L.key1 = take(8 * m);
-    L.grp = take(4 * m);
+    L.grp = take(4 * (m + 64));  // grp and aux2 trade places every pass
     L.aux1 = take(4 * m);
     L.aux2 = take(4 * (m + 64));
     L.rankScratch = take(4 * radixScratchWords(m));
