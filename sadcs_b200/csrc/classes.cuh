@@ -100,8 +100,7 @@ inline uint32_t* classErrorWord(uint32_t* scratch, uint32_t texts) {
 }
 
 // Class 0: the live sample positions in rank order, the ranks in [lo, hi) of them. The writes land
-// at random places of the list, so the caller covers the ranks in slices whose part of the list
-// stays in L2 (a 4-byte write to a line that is not there costs a DRAM read and write of its sector).
+// at random places of the list, so the caller covers the ranks in slices of the list (kRankSlice).
 __global__ void classScatterSample(const uint32_t* __restrict__ ranks, uint32_t slots, uint32_t lo, uint32_t hi,
                                    TextSet texts, uint32_t* __restrict__ list) {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -112,9 +111,6 @@ __global__ void classScatterSample(const uint32_t* __restrict__ ranks, uint32_t 
     if (p >= texts.endOf(p)) return;  // past the end, or between texts
     list[r] = p;
 }
-
-// Ranks per slice of classScatterSample: 12M ranks = 48 MB of list.
-constexpr uint32_t kScatterSlice = 12u << 20;
 
 // Codes of the 8 characters before p: byte i holds the code of T[p - 1 - i] (0 before position 0),
 // from one 64-bit window of the code stream (b <= 8, so 8 codes fit in it).
@@ -233,8 +229,10 @@ inline cudaError_t sortClasses(uint32_t total, const TextSet& texts, const uint3
                                uint64_t* const chains[2], cudaStream_t stream) {
     const uint32_t J = tables.texts;
     const uint32_t live = plan.start[1];
-    for (uint32_t lo = 0; lo < live; lo += kScatterSlice) {
-        const uint32_t hi = live - lo > kScatterSlice ? lo + kScatterSlice : live;
+    // Each slice reads every rank once: past kMaxRankSlices slices one plain pass costs less.
+    const uint32_t slice = ceilDiv(live, kRankSlice) <= kMaxRankSlices ? kRankSlice : live;
+    for (uint32_t lo = 0; lo < live; lo += slice) {
+        const uint32_t hi = live - lo > slice ? lo + slice : live;
         SADCS_TRY(launch(classScatterSample, (slots + 255) / 256, 256, 0, stream, ranks, slots, lo, hi, texts, lists));
     }
     uint32_t* hist = scratch;  // [kClasses][J][256]

@@ -135,14 +135,42 @@ __device__ __forceinline__ void refineFlags(const uint32_t* __restrict__ grp, co
                                             uint32_t& next, uint32_t& keep) {
     uint32_t prevG = base > 0 && base - 1 < u ? grp[base - 1] : 0xFFFFFFFFu;
     uint64_t prevK = base > 0 && base - 1 < u ? key[base - 1] : 0;
+    // The thread's 16 elements by 16-byte loads (base is a multiple of 16 and the buffers are
+    // 256-byte aligned), and the one after them.
+    uint32_t gv[kRefineItems + 1];
+    uint64_t kv[kRefineItems + 1];
+    if (base + kRefineItems < u) {
+#pragma unroll
+        for (int q = 0; q < kRefineItems / 4; q++) {
+            const uint4 v = *reinterpret_cast<const uint4*>(grp + base + 4 * q);
+            gv[4 * q] = v.x;
+            gv[4 * q + 1] = v.y;
+            gv[4 * q + 2] = v.z;
+            gv[4 * q + 3] = v.w;
+        }
+#pragma unroll
+        for (int q = 0; q < kRefineItems / 2; q++) {
+            const ulonglong2 v = *reinterpret_cast<const ulonglong2*>(key + base + 2 * q);
+            kv[2 * q] = v.x;
+            kv[2 * q + 1] = v.y;
+        }
+        gv[kRefineItems] = grp[base + kRefineItems];
+        kv[kRefineItems] = key[base + kRefineItems];
+    } else {
+#pragma unroll
+        for (int k = 0; k <= kRefineItems; k++) {
+            gv[k] = base + k < u ? grp[base + k] : 0;
+            kv[k] = base + k < u ? key[base + k] : 0;
+        }
+    }
     old = 0;
     next = 0;
 #pragma unroll
     for (int k = 0; k <= kRefineItems; k++) {
         const uint32_t e = base + k;
         if (e >= u) break;
-        const uint32_t ge = grp[e];
-        const uint64_t ke = key[e];
+        const uint32_t ge = gv[k];
+        const uint64_t ke = kv[k];
         const bool startOld = e == 0 || ge != prevG;
         if (k < kRefineItems) {
             g[k] = ge;
@@ -262,13 +290,27 @@ __global__ void __launch_bounds__(kRefineThreads) rankRefineApply(const uint32_t
     uint32_t runOld = max(agg[blockIdx.x], threadIdx.x ? incOld[threadIdx.x - 1] : 0u);
     uint32_t runNew = max(agg[tiles + blockIdx.x], threadIdx.x ? incNew[threadIdx.x - 1] : 0u);
     uint32_t at = agg[2 * tiles + blockIdx.x] + ic - kept;
+    uint32_t items[kRefineItems];
+    if (base + kRefineItems <= u) {
+#pragma unroll
+        for (int q = 0; q < kRefineItems / 4; q++) {
+            const uint4 v = *reinterpret_cast<const uint4*>(lst + base + 4 * q);
+            items[4 * q] = v.x;
+            items[4 * q + 1] = v.y;
+            items[4 * q + 2] = v.z;
+            items[4 * q + 3] = v.w;
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < kRefineItems; k++) items[k] = base + k < u ? lst[base + k] : 0;
+    }
 #pragma unroll
     for (int k = 0; k < kRefineItems; k++) {
         const uint32_t e = base + k;
         if (e >= u) break;
         if ((old >> k) & 1) runOld = e;
         if ((next >> k) & 1) runNew = e;
-        const uint32_t item = lst[e];
+        const uint32_t item = items[k];
         const uint32_t id = g[k] + (runNew - runOld);
         const bool kept = (keep >> k) & 1;
         if (item < slots && (!kept || writeAll)) ranks[item] = id;
