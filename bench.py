@@ -417,7 +417,8 @@ def run_ours(args, world, rank, local) -> None:
     traffic = profile_traffic(args.workload)
     if traffic:
         roofline["traffic"] = round(traffic * n)
-        roofline["traffic_source"] = "ncu dram__bytes_read.sum + dram__bytes_write.sum, per input byte, scaled"
+        roofline["traffic_source"] = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the final merge on this "
+                                      "workload, per input byte (profiles/traffic.json), times n")
     line = {"metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms_max, 3), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u8", "data": "synthetic",
