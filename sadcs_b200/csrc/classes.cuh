@@ -9,8 +9,9 @@
 //
 // Several texts: each global class list is the texts' class lists one after another (text order),
 // and each text is a segment of the pass: a segmented onesweep pass sorts all texts at once, every
-// text from its own digit bases. The walk, the filter, the character gather and the stable
-// counting sort are that one pass; the digit bases come from one streaming read of the text.
+// text from its own digit bases. The walk, the filter and the stable counting sort are that one
+// pass, keyed by the character each element carries (ClassLoader); the digit bases come from one
+// streaming read of the text.
 #pragma once
 
 #include <algorithm>

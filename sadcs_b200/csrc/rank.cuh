@@ -2,14 +2,15 @@
 // src/cuda/samplerank.cuh; the result is the same rank array, gpusa.h:62-73).
 //
 // State: a list of the unresolved sample suffixes (compact sample indices t, position
-// (t/7)*32 + D[t%7]) kept in group order, and for every sample its group id in the rank array:
-// the number of sample suffixes known to be smaller than every member of its group, which is the
-// final rank once the group is a singleton.
+// (t/7)*32 + D[t%7]) kept in group order, with each element's group id beside it: the number of
+// sample suffixes known to be smaller than every member of its group, which is the final rank once
+// the group is a singleton. The rank array (indexed by t) holds the final ranks of the resolved
+// samples and, from the pass before the first doubling round on, the ids of all listed ones.
 //
-// One pass: key every listed suffix by a subkey, sort the list stably by (group id, subkey), split
-// groups where the subkey changes (a new group's id is its old id plus its offset inside the old
-// group, from the last old and new group heads before each element), write the ids, and compact
-// away the singletons (three fused kernels per pass, below).
+// One pass: key every listed suffix by a subkey, sort the list by (group id, subkey), split groups
+// where the subkey changes (a new group's id is its old id plus its offset inside the old group,
+// from the last old and new group heads before each element), write the ids, and compact away the
+// singletons (three fused kernels per pass, below).
 //   character passes: the keyChars codes at p + depth (alphabet.cuh: 29 for DNA, 10 for 6-bit text,
 //     7 for bytes) in the top bits and min(remaining, keyChars) in the low tag bits (code 0 at or
 //     past the end), so a suffix that ends inside the window is separated from every longer one
@@ -338,12 +339,6 @@ struct RankStats {
     int characterPasses = 0;
     int doublingRounds = 0;
 };
-
-__global__ void rankGatherGroupKeys(const uint32_t* __restrict__ ranks, const uint32_t* __restrict__ lst,
-                                    uint64_t* __restrict__ key, uint32_t u, uint32_t m) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < u) key[i] = lst[i] < m ? ranks[lst[i]] : 0;
-}
 
 // Ranks the live sample suffixes of the texts. slots = rank entries (sample positions of the whole
 // concatenation); live = live samples; sampleBase (device, per text) is used with several texts.
