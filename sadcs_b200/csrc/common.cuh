@@ -9,6 +9,7 @@
 // 16-byte window at any position <= n + 31 stays inside the buffer and reads zeros past the end.
 #pragma once
 
+#include <atomic>
 #include <cstddef>
 #include <cstdint>
 #include <utility>
@@ -219,6 +220,22 @@ inline cudaError_t launch(void (*kernel)(Params...), dim3 grid, dim3 block, size
     kernel<<<grid, block, shared, stream>>>(std::forward<Args>(args)...);
     ++tLaunches;
     return cudaGetLastError();
+}
+
+// Runs set() (a kernel's function attributes) the first time a call site meets the current device;
+// `configured` is the call site's set of devices done. The server's worker threads reach the same
+// call sites at once, so the set is atomic; two threads may both run set(), which is harmless (the
+// attributes are the same), and a thread sees a device as done only after its set() returned.
+template <class Set>
+inline cudaError_t configureOnce(std::atomic<uint64_t>& configured, Set set) {
+    int device = 0;
+    cudaError_t error = cudaGetDevice(&device);
+    if (error != cudaSuccess) return error;
+    const uint64_t bit = uint64_t(1) << (device & 63);
+    if (configured.load(std::memory_order_acquire) & bit) return cudaSuccess;
+    if ((error = set()) != cudaSuccess) return error;
+    configured.fetch_or(bit, std::memory_order_acq_rel);
+    return cudaSuccess;
 }
 
 }  // namespace sadcs

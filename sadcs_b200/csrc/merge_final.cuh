@@ -360,18 +360,16 @@ __global__ void __launch_bounds__(kMergeThreads) mergeTree(MergeArgs a) {
 template <int W, bool kMulti, bool kFinal>
 inline cudaError_t launchTreeFor(const MergeArgs& args, uint32_t tiles, cudaStream_t stream) {
     constexpr size_t shared = FinalTile<W, kMulti>::sharedBytes();
-    static uint64_t configured = 0;
-    int device = 0;
-    SADCS_TRY(cudaGetDevice(&device));
-    if (!(configured >> (device & 63) & 1)) {
+    static std::atomic<uint64_t> configured{0};
+    SADCS_TRY(configureOnce(configured, [] {
         SADCS_TRY(cudaFuncSetAttribute(mergeTree<W, kMulti, kFinal>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(shared)));
 #if SADCS_MERGE_CARVEOUT >= 0
         SADCS_TRY(cudaFuncSetAttribute(mergeTree<W, kMulti, kFinal>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                        SADCS_MERGE_CARVEOUT));
 #endif
-        configured |= uint64_t(1) << (device & 63);
-    }
+        return cudaSuccess;
+    }));
     return launch(mergeTree<W, kMulti, kFinal>, tiles, kMergeThreads, shared, stream, args);
 }
 

@@ -525,14 +525,11 @@ cudaError_t radixOnesweepPass(const Loader& ld, const Storer& st, const Segments
     SADCS_TRY(cudaMemsetAsync(scratch.control, 0, 4, stream));
     constexpr size_t shared = radixSharedBytes(sizeof(Key));
     // The opt-in above 48 KiB of dynamic shared memory is per function and per device.
-    static uint64_t configured = 0;
-    int device = 0;
-    SADCS_TRY(cudaGetDevice(&device));
-    if (!(configured >> (device & 63) & 1)) {
-        SADCS_TRY(cudaFuncSetAttribute(radixOnesweep<Key, Loader, Storer, Segments>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(shared)));
-        configured |= uint64_t(1) << (device & 63);
-    }
+    static std::atomic<uint64_t> configured{0};
+    SADCS_TRY(configureOnce(configured, [] {
+        return cudaFuncSetAttribute(radixOnesweep<Key, Loader, Storer, Segments>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(shared));
+    }));
     return launch(radixOnesweep<Key, Loader, Storer, Segments>, tiles, kSortThreads, shared, stream, ld, st, segs,
                   digitBase, scratch.status, scratch.control, scratch.control + 1);
 }

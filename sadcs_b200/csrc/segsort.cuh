@@ -347,14 +347,11 @@ inline cudaError_t segmentedSort(const uint32_t* grp, uint32_t u, uint64_t* keys
     const uint32_t big = hostWords[1], bigTiles = hostWords[2];
 
     // Small segments, in place.
-    static uint64_t configured = 0;
-    int device = 0;
-    SADCS_TRY(cudaGetDevice(&device));
-    if (!(configured >> (device & 63) & 1)) {
-        SADCS_TRY(cudaFuncSetAttribute(segSortSmall, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       static_cast<int>(segSortSharedBytes())));
-        configured |= uint64_t(1) << (device & 63);
-    }
+    static std::atomic<uint64_t> configured{0};
+    SADCS_TRY(configureOnce(configured, [] {
+        return cudaFuncSetAttribute(segSortSmall, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(segSortSharedBytes()));
+    }));
     SADCS_TRY(launch(segSortSmall, ceilDiv(u, kSegChunk), kSegThreads, segSortSharedBytes(), stream, b.heads,
                      segments, keys, vals, keys, vals, keyBits));
     if (big == 0) return cudaSuccess;
