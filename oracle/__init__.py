@@ -73,6 +73,8 @@ def lib() -> ctypes.CDLL:
         L.oracle_check_sa.argtypes = [_u8p, ctypes.c_int64, _u32p, _i64p]
         L.oracle_check_bwt.restype = ctypes.c_int
         L.oracle_check_bwt.argtypes = [_u8p, ctypes.c_int64, _u8p, ctypes.c_int64, _i64p]
+        L.oracle_lcp.restype = ctypes.c_int
+        L.oracle_lcp.argtypes = [_u8p, ctypes.c_int64, _u32p, _u32p]
         L.oracle_cover_tables.restype = None
         L.oracle_cover_tables.argtypes = [_u8p, _u8p, _u8p]
         _lib = L
@@ -295,6 +297,17 @@ def bwt_from_sa(text, sa: np.ndarray):
     bwt = np.zeros(max(n, 1), np.uint8)
     primary = lib().oracle_bwt_from_sa(_ptr(_nonempty(t), _u8p), n, _ptr(_nonempty(sa), _u32p), _ptr(bwt, _u8p))
     return bwt[:n], int(primary)
+
+
+def lcp(text, sa: np.ndarray) -> np.ndarray:
+    """lcp[0] = 0, lcp[r] = common prefix length of suffixes sa[r - 1] and sa[r] (uint32)."""
+    t = _text(text)
+    n = len(t)
+    sa = np.ascontiguousarray(sa, dtype=np.uint32)
+    out = np.zeros(max(n, 1), np.uint32)
+    if not lib().oracle_lcp(_ptr(_nonempty(t), _u8p), n, _ptr(_nonempty(sa), _u32p), _ptr(out, _u32p)):
+        raise MemoryError("oracle_lcp")
+    return out[:n]
 
 
 def check_sa(text, sa: np.ndarray):

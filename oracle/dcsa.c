@@ -547,3 +547,43 @@ int oracle_check_bwt(const uint8_t* text, int64_t n, const uint8_t* bwt, int64_t
     }
     return 1;
 }
+
+/* ---- LCP array (no counterpart in the reference) ---------------------------------------- */
+
+int oracle_lcp(const uint8_t* text, int64_t n, const uint32_t* sa, uint32_t* lcp) {
+    if (n <= 0) {
+        return 1;
+    }
+    /* phi[p] = the suffix just before suffix p in suffix order (n for the smallest suffix); then
+     * plcp[p] = lcp(p, phi[p]) in text order, where plcp[p + 1] >= plcp[p] - 1 lets the common
+     * length carry from one position to the next (linear total work). */
+    uint32_t* phi = malloc((size_t)n * sizeof(uint32_t));
+    if (!phi) {
+        return 0;
+    }
+    phi[sa[0]] = (uint32_t)n;
+    for (int64_t r = 1; r < n; r++) {
+        phi[sa[r]] = sa[r - 1];
+    }
+    int64_t h = 0;
+    for (int64_t p = 0; p < n; p++) {
+        const int64_t q = phi[p];
+        if (q == n) {
+            h = 0;
+            phi[p] = 0;
+            continue;
+        }
+        while (p + h < n && q + h < n && text[p + h] == text[q + h]) {
+            h++;
+        }
+        phi[p] = (uint32_t)h; /* phi[p] is not read again: it becomes plcp[p] */
+        if (h > 0) {
+            h--;
+        }
+    }
+    for (int64_t r = 0; r < n; r++) {
+        lcp[r] = phi[sa[r]];
+    }
+    free(phi);
+    return 1;
+}

@@ -22,6 +22,10 @@
  *   oracle_sample_ranks_from_sa src/cuda/gpusa.h:65-73
  *   oracle_check_sa            src/common/checker.cpp:53-109 (checkFast), in 64-bit arithmetic
  *   oracle_check_bwt           src/common/checker.cpp:196-245 (LF inversion), in 64-bit arithmetic
+ *   oracle_lcp                 no counterpart (the reference computes no LCP array): Kasai, Lee,
+ *                              Arimura, Arikawa and Park's linear-time LCP, in the Phi-array
+ *                              formulation (Karkkainen, Manzini and Puglisi), pinned by the definition
+ *                              (tests/test_oracle.py compares it with direct comparison of neighbours)
  *
  * Parity pinning: tests/golden/ holds outputs of the reference's own CPU build (oracle/_ref), made by
  * tests/golden/make_golden.py; tests/test_oracle.py checks every function here against them.
@@ -57,6 +61,10 @@ int64_t oracle_bwt_from_sa(const uint8_t* text, int64_t n, const uint32_t* sa, u
 /* Return 1 if correct; *index gets the first failing SA index (or text position for the BWT), -1 if ok. */
 int oracle_check_sa(const uint8_t* text, int64_t n, const uint32_t* sa, int64_t* index);
 int oracle_check_bwt(const uint8_t* text, int64_t n, const uint8_t* bwt, int64_t primary, int64_t* index);
+
+/* lcp[0] = 0 and lcp[r] = the length of the longest common prefix of suffixes sa[r - 1] and sa[r]
+ * (r >= 1), for the suffix array sa of text. Returns 0 if memory runs out. */
+int oracle_lcp(const uint8_t* text, int64_t n, const uint32_t* sa, uint32_t* lcp);
 
 #ifdef __cplusplus
 }

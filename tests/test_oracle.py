@@ -116,3 +116,28 @@ def test_oracle_vs_reference_random():
         for _ in range(4):
             text = W.random_text(rng, 1 + int(rng.below(20000)[0]), sigma)
             assert np.array_equal(oracle.dc_sa(text), oracle.ref_sa(text).astype(np.uint32))
+
+
+def _naive_lcp(text: np.ndarray, sa: np.ndarray) -> np.ndarray:
+    out = np.zeros(len(sa), np.uint32)
+    for r in range(1, len(sa)):
+        a, b = text[int(sa[r - 1]):], text[int(sa[r]):]
+        m = min(len(a), len(b))
+        differ = np.flatnonzero(a[:m] != b[:m])
+        out[r] = differ[0] if len(differ) else m
+    return out
+
+
+def test_lcp_oracle_matches_the_definition():
+    """oracle.lcp (Kasai over the Phi array; no reference counterpart) against direct comparison of
+    every pair of neighbouring suffixes, on the golden inputs and on run, Fibonacci and natural text."""
+    texts = [text for _, text in SMALL]
+    texts += [W.run_text(3000), W.fibonacci_text(4000), W.natural_text(6000, seed=4),
+              np.frombuffer(b"mississippi", np.uint8), np.frombuffer(b"a", np.uint8)]
+    for text in texts:
+        text = np.ascontiguousarray(text, dtype=np.uint8)
+        if len(text) == 0 or len(text) > 20000:
+            continue
+        sa = oracle.naive_sa(text)
+        assert np.array_equal(oracle.lcp(text, sa), _naive_lcp(text, sa))
+    assert len(oracle.lcp(np.zeros(0, np.uint8), np.zeros(0, np.uint32))) == 0
