@@ -218,6 +218,15 @@ int sadcs_gpu_check_bwt(const uint8_t* d_text, int64_t n, const uint8_t* d_bwt, 
  * Returns SADCS_FAILED if d_bwt is not a valid BWT. */
 int sadcs_gpu_inverse_bwt(const uint8_t* d_bwt, int64_t n, int64_t primary, uint8_t* d_text, void* stream);
 
+/* No counterpart (the reference computes no LCP array): the longest-common-prefix array of a suffix
+ * array on the device. lcp[0] = 0 and lcp[r] = the length of the longest common prefix of suffixes
+ * d_sa[r - 1] and d_sa[r], for d_sa (n uint32 entries) the suffix array of d_text (n bytes, no
+ * padding needed), n up to 2^32 - 256. d_lcp gets n uint32 entries and may be d_sa itself (the
+ * suffix array is then replaced by its LCP array). Uses about 4.13n bytes of temporary device memory;
+ * returns when the array is complete. A d_sa that is not the suffix array of d_text gives an
+ * unspecified d_lcp, never a read outside the buffers. */
+int sadcs_gpu_lcp(const uint8_t* d_text, int64_t n, const uint32_t* d_sa, uint32_t* d_lcp, void* stream);
+
 /* No counterpart: the capacity (bytes of text) of a context. */
 int64_t sadcs_gpu_context_capacity(const sadcs_gpu_context* context);
 

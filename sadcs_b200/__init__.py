@@ -160,6 +160,8 @@ def lib() -> ctypes.CDLL:
         L.sadcs_gpu_check_suffix_array_static.restype = ctypes.c_int
         L.sadcs_gpu_check_suffix_array_static.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, _i64p,
                                                           ctypes.POINTER(ctypes.c_char_p), ctypes.c_void_p]
+        L.sadcs_gpu_lcp.restype = ctypes.c_int
+        L.sadcs_gpu_lcp.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
         _lib = L
     return _lib
 
@@ -399,6 +401,13 @@ def inverse_bwt_device(d_bwt: int, n: int, primary: int, d_text: int, stream: in
     """unbwt on device buffers: d_text (n bytes) from the BWT and its primary index."""
     _check(lib().sadcs_gpu_inverse_bwt(ctypes.c_void_p(d_bwt), int(n), int(primary), ctypes.c_void_p(d_text),
                                        ctypes.c_void_p(stream) if stream else None))
+
+
+def lcp_device(d_text: int, n: int, d_sa: int, d_lcp: int, stream: int | None = None) -> None:
+    """The LCP array of a device suffix array (sadcs_gpu_lcp): d_lcp[0] = 0 and d_lcp[r] = the
+    longest common prefix of suffixes d_sa[r - 1] and d_sa[r] (n uint32 entries; d_lcp may be d_sa)."""
+    _check(lib().sadcs_gpu_lcp(ctypes.c_void_p(d_text), int(n), ctypes.c_void_p(d_sa), ctypes.c_void_p(d_lcp),
+                               ctypes.c_void_p(stream) if stream else None))
 
 
 def allocate_pinned(nbytes: int) -> np.ndarray:

@@ -24,6 +24,7 @@
 #include "check.cuh"
 #include "classes.cuh"
 #include "common.cuh"
+#include "lcp.cuh"
 #include "merge.cuh"
 #include "merge_final.cuh"
 #include "primitives.cuh"
@@ -1218,6 +1219,24 @@ int sadcs_gpu_check_bwt(const uint8_t* d_text, int64_t n, const uint8_t* d_bwt, 
     cudaFreeAsync(word, st);
     cudaStreamSynchronize(st);
     return status;
+}
+
+int sadcs_gpu_lcp(const uint8_t* d_text, int64_t n, const uint32_t* d_sa, uint32_t* d_lcp, void* stream) {
+    tLastError[0] = '\0';
+    if (n <= 0) return SADCS_OK;
+    if (n > kMaxText) {
+        setError("text of %lld bytes exceeds the limit of %lld", static_cast<long long>(n), static_cast<long long>(kMaxText));
+        return SADCS_FAILED;
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    uint32_t* scratch = nullptr;
+    cudaError_t error = cudaMallocAsync(&scratch, 4 * lcp::scratchWords(static_cast<uint64_t>(n)), st);
+    if (error != cudaSuccess) return failed("cudaMallocAsync", error);
+    error = lcp::lcpArray(d_text, static_cast<uint32_t>(n), d_sa, d_lcp, scratch, st);
+    cudaFreeAsync(scratch, st);
+    const cudaError_t done = cudaStreamSynchronize(st);
+    if (error == cudaSuccess) error = done;
+    return error == cudaSuccess ? SADCS_OK : failed("LCP array", error);
 }
 
 int sadcs_gpu_rank_sample(const uint8_t* text, int64_t n, uint32_t* ranks, sadcs_gpu_stats* stats) {
