@@ -1,6 +1,7 @@
 """bench.py - suffix array + BWT construction throughput on B200, and the reference CPU arm.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--workload natural256m|uniform8m|genome3g]
+    python bench.py --workload batch4096 | serve | lcp256m    batched, served, LCP array from text + SA
     python bench.py --impl reference ...       the reference's CPU variant on the host cores
     python bench.py --impl reference-gpu ...   the reference's own CUDA build on this GPU
 
@@ -42,6 +43,9 @@ UNIT = "MiB/s"
 MIB = float(1 << 20)
 PIPELINE_BYTES_PER_INPUT_BYTE = 82.125
 MERGE_BYTES_PER_INPUT_BYTE = 53.0
+# LCP array (sadcs_gpu_lcp), per position: Phi scatter 4 + 4, irreducible test 4 + 1 + 1 + 4 (the
+# character comparisons are not credited), max-scan 4 + 4, gather 4 + 4 + 4.
+LCP_BYTES_PER_POSITION = 38.0
 FALLBACK_HBM_GBS = 6650.0
 
 BATCH_DESC = ("4096 texts, lengths log-uniform in [1 KiB, 4 MiB], thirds over {A,C,G,T}, a 20-letter protein-like "
@@ -529,6 +533,85 @@ def profile_traffic(workload: str):
         return None
 
 
+def scan_launches(count: int) -> int:
+    """Kernels of the library's device-wide scan of count elements (primitives.cuh deviceScan)."""
+    if count == 0:
+        return 0
+    blocks = -(-count // 4096)
+    return 1 if blocks == 1 else 2 + scan_launches(blocks)
+
+
+def run_lcp(args, world, rank, local) -> None:
+    """The LCP array of the natural256m text's suffix array (sadcs_gpu_lcp) on device buffers; the
+    suffix array is built once, outside the timed region. Each step is one call, its scratch
+    allocation (stream-ordered) included."""
+    import torch
+
+    import oracle
+    import sadcs_b200 as sa
+    from sadcs_b200 import workloads as W
+
+    torch.cuda.set_device(local)
+    desc, gen = WORKLOADS["natural256m"]
+    text = gen(W)
+    n = int(len(text))
+    props = torch.cuda.get_device_properties(local)
+    uuid = getattr(props, "uuid", None)
+    uuid = f"GPU-{uuid}" if uuid is not None and not str(uuid).startswith("GPU-") else (str(uuid) if uuid else None)
+    device = f"cuda:{local}"
+    d_text = torch.from_numpy(text).to(device)
+    d_sa = torch.empty(n, dtype=torch.int32, device=device)
+    d_lcp = torch.empty(n, dtype=torch.int32, device=device)
+    stream = torch.cuda.current_stream()
+    handle = stream.cuda_stream
+    sa.build_device(d_text.data_ptr(), n, d_sa.data_ptr(), None, stream=handle)
+
+    def step():
+        sa.lcp_device(d_text.data_ptr(), n, d_sa.data_ptr(), d_lcp.data_ptr(), stream=handle)
+
+    for _ in range(max(args.warmup, 0)):
+        step()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(uuid)
+    sampler.start()
+    time.sleep(0.3)
+    barrier(world)
+    torch.cuda.synchronize()
+    start = torch.cuda.Event(enable_timing=True)
+    stop = torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    for _ in range(args.steps):
+        step()
+    stop.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    clocks = sampler.stop()
+    ms = start.elapsed_time(stop) / args.steps
+    ms_max = max_over_ranks(ms, world)
+    value = sum_over_ranks(float(n), world) / MIB / (ms_max / 1e3)
+    verified = None
+    if args.verify:
+        h_sa = d_sa.cpu().numpy().view(np.uint32)
+        verified = bool(np.array_equal(d_lcp.cpu().numpy().view(np.uint32), oracle.lcp(text, h_sa)))
+    if rank != 0:
+        return
+    peak, peak_kind = hbm_peak()
+    gbs = LCP_BYTES_PER_POSITION * n / (ms / 1e3) / 1e9
+    line = {"metric": "input MB/s (LCP array from text + SA)", "value": round(value, 3), "unit": UNIT,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_max, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": {"workload": "lcp256m", "description": desc, "text_bytes": n,
+                       "outputs": "LCP (uint32) from device text + SA", "l2": "inputs larger than L2",
+                       "parallelism": "replicas" if world > 1 else "single GPU"},
+            "roofline": {"bound": "hbm", "kernel": "all LCP passes of one call (Phi, irreducible test, warp "
+                         "pass, max-scan, gather)", "achieved": round(gbs, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(gbs / peak, 4), "traffic": None,
+                         "algorithmic_bytes_per_input_byte": LCP_BYTES_PER_POSITION,
+                         "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"},
+            "clocks": clocks, "gpu_launches": args.steps * (4 + scan_launches(n)), "verified": verified}
+    print(json.dumps(line), flush=True)
+
+
 def run_batch(args, world, rank, local) -> None:
     """Config 4: many uneven texts in one construction, against one construction per text."""
     import torch
@@ -761,7 +844,7 @@ def main() -> None:
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference", "reference-gpu"], default="ours")
-    p.add_argument("--workload", choices=sorted(WORKLOADS) + ["batch4096", "serve"], default="natural256m")
+    p.add_argument("--workload", choices=sorted(WORKLOADS) + ["batch4096", "serve", "lcp256m"], default="natural256m")
     p.add_argument("--batch-count", type=int, default=4096)
     p.add_argument("--plain-sample", type=int, default=64)
     p.add_argument("--serve-loads", default="50,200,800")
@@ -782,7 +865,10 @@ def main() -> None:
         # Rank 0 alone times the reference on the host cores; other ranks exit without work (and
         # without joining a process group, so nothing waits on them).
         world, rank, _ = rank_env()
-        if args.workload in ("batch4096", "serve"):
+        if args.workload == "lcp256m":
+            if rank == 0:
+                print(json.dumps({"impl": "reference", "unavailable": "the reference computes no LCP array"}))
+        elif args.workload in ("batch4096", "serve"):
             if rank == 0:
                 print(json.dumps({"impl": "reference", "unavailable": "the reference has no batched or served "
                                   "construction (one text per call); its per-text CPU rate is the natural256m line"}))
@@ -795,6 +881,8 @@ def main() -> None:
             run_batch(args, world, rank, local)
         elif args.workload == "serve":
             run_serve(args, world, rank, local)
+        elif args.workload == "lcp256m":
+            run_lcp(args, world, rank, local)
         else:
             run_ours(args, world, rank, local)
     finally:
