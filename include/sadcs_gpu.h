@@ -201,10 +201,20 @@ int sadcs_gpu_server_create(int64_t memory_budget, int32_t workers, int64_t smal
 int sadcs_gpu_server_submit(sadcs_gpu_server* server, const uint8_t* text, int64_t n, uint32_t* sa, uint8_t* bwt,
                             uint64_t* ticket);
 /* Blocks until the request is done (timeout_seconds < 0: no limit); latency gets queued, device and
- * total seconds; batch_size the number of requests built together with it. */
+ * total seconds; batch_size the number of requests built together with it. A ticket is waited for
+ * once, by one thread: the wait that returns its result also forgets it. */
 int sadcs_gpu_server_wait(sadcs_gpu_server* server, uint64_t ticket, double timeout_seconds, int64_t* primary,
                           double* latency, int32_t* batch_size);
 void sadcs_gpu_server_counters(sadcs_gpu_server* server, int64_t* constructions, int64_t* launches);
+/* Cancels a request that no worker has taken yet: returns SADCS_OK, and its wait returns SADCS_FAILED
+ * with "cancelled". A request already being built or done, or an unknown ticket, gives SADCS_FAILED
+ * and the request is left as it is. */
+int sadcs_gpu_server_cancel(sadcs_gpu_server* server, uint64_t ticket);
+/* Fault injection for tests of the error path: the next `count` constructions fail their device
+ * allocation as the memory pool does when it is out of memory (a fake of cudaMallocFromPoolAsync
+ * returning cudaErrorMemoryAllocation; nothing is allocated). Their requests complete with
+ * SADCS_NOT_ENOUGH_MEMORY and the server goes on serving the others. */
+void sadcs_gpu_server_fail_allocations(sadcs_gpu_server* server, int64_t count);
 void sadcs_gpu_server_destroy(sadcs_gpu_server* server);
 
 /* No counterpart: the reference's BWT check (src/common/checker.cpp:196-245) on the device: inverts

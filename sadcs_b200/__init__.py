@@ -148,6 +148,10 @@ def lib() -> ctypes.CDLL:
         L.sadcs_gpu_server_counters.argtypes = [ctypes.c_void_p, _i64p, _i64p]
         L.sadcs_gpu_server_destroy.restype = None
         L.sadcs_gpu_server_destroy.argtypes = [ctypes.c_void_p]
+        L.sadcs_gpu_server_cancel.restype = ctypes.c_int
+        L.sadcs_gpu_server_cancel.argtypes = [ctypes.c_void_p, ctypes.c_uint64]
+        L.sadcs_gpu_server_fail_allocations.restype = None
+        L.sadcs_gpu_server_fail_allocations.argtypes = [ctypes.c_void_p, ctypes.c_int64]
         L.sadcs_gpu_check_bwt.restype = ctypes.c_int
         L.sadcs_gpu_check_bwt.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64, _i64p,
                                           ctypes.c_void_p]
@@ -468,6 +472,16 @@ class Server:
         t, sa, out, n = self._pending.pop(ticket)
         _check(status)
         return sa[:n], out[:n], int(primary.value), tuple(latency), int(batch.value)
+
+    def cancel(self, ticket: int) -> bool:
+        """Cancels a request no worker has taken yet (True); its wait then raises GpuError
+        ("cancelled"). False when it is being built, done, or unknown."""
+        return lib().sadcs_gpu_server_cancel(self._handle, int(ticket)) == GpuStatus.Ok
+
+    def fail_allocations(self, count: int) -> None:
+        """Fault injection: the next `count` constructions fail their device allocation as an
+        exhausted pool would; their requests raise GpuError (NotEnoughMemory)."""
+        lib().sadcs_gpu_server_fail_allocations(self._handle, int(count))
 
     def counters(self):
         c, l = ctypes.c_int64(0), ctypes.c_int64(0)

@@ -67,9 +67,19 @@ struct sadcs_gpu_server {
     std::unordered_map<uint64_t, ServerRequest*> requests;
     std::vector<std::thread> threads;
     uint64_t launches = 0, constructions = 0;
+    std::atomic<int64_t> failAllocations{0};  // constructions left whose slab allocation is made to fail
 };
 
 namespace {
+
+// True (and one fewer left) while sadcs_gpu_server_fail_allocations has failures pending.
+bool takeInjectedFailure(sadcs_gpu_server* srv) {
+    int64_t pending = srv->failAllocations.load();
+    while (pending > 0) {
+        if (srv->failAllocations.compare_exchange_weak(pending, pending - 1)) return true;
+    }
+    return false;
+}
 
 // Footprint of a construction: its planned peak on the device.
 size_t footprintOf(const Batch& b) {
@@ -84,7 +94,9 @@ void serveBatch(sadcs_gpu_server* srv, sadcs_gpu_context& ctx, std::vector<Serve
     const double started = nowSeconds();
     double constructed = started;
     for (ServerRequest* r : group) r->started = started;
-    cudaError_t error = cudaMallocFromPoolAsync(reinterpret_cast<void**>(&ctx.slab), footprint, srv->pool, ctx.stream);
+    cudaError_t error = takeInjectedFailure(srv) ? cudaErrorMemoryAllocation
+                                                 : cudaMallocFromPoolAsync(reinterpret_cast<void**>(&ctx.slab),
+                                                                           footprint, srv->pool, ctx.stream);
     if (error != cudaSuccess) {
         status = failed("allocating from the pool", error);
         message = tLastError;
@@ -369,6 +381,41 @@ int sadcs_gpu_server_wait(sadcs_gpu_server* srv, uint64_t ticket, double timeout
     srv->requests.erase(it);
     delete r;
     return status;
+}
+
+// Takes a request that no worker has taken yet out of the queue; its wait then returns
+// SADCS_FAILED with "cancelled". A request being built, done or unknown is left as it is.
+int sadcs_gpu_server_cancel(sadcs_gpu_server* srv, uint64_t ticket) {
+    tLastError[0] = '\0';
+    if (!srv) {
+        setError("server is null");
+        return SADCS_FAILED;
+    }
+    std::lock_guard<std::mutex> lock(srv->mu);
+    auto it = srv->requests.find(ticket);
+    if (it == srv->requests.end()) {
+        setError("unknown ticket %llu", static_cast<unsigned long long>(ticket));
+        return SADCS_FAILED;
+    }
+    ServerRequest* r = it->second;
+    auto queued = std::find(srv->queue.begin(), srv->queue.end(), r);
+    if (queued == srv->queue.end()) {
+        setError(r->done ? "request already done" : "request already being built");
+        return SADCS_FAILED;
+    }
+    srv->queue.erase(queued);
+    r->status = SADCS_FAILED;
+    r->error = "cancelled";
+    r->started = r->finished = nowSeconds();
+    r->done = true;
+    srv->finished.notify_all();
+    srv->work.notify_all();  // the queue's head, and so what can be admitted, may have changed
+    return SADCS_OK;
+}
+
+// The next `count` constructions fail their slab allocation as the pool would when out of memory.
+void sadcs_gpu_server_fail_allocations(sadcs_gpu_server* srv, int64_t count) {
+    if (srv) srv->failAllocations.store(count > 0 ? count : 0);
 }
 
 // Constructions run and kernels launched so far.
