@@ -41,13 +41,47 @@ def _files(path: Path, recursive: bool):
 
 
 def _load(path) -> np.ndarray:
-    return np.fromfile(path, dtype=np.uint8)
+    """A regular input file memory-mapped read-only: no copy into process memory; the
+    construction's upload reads the pages straight from the mapping. Anything else (a pipe) is
+    read in full."""
+    if not os.path.isfile(path):
+        return np.fromfile(path, dtype=np.uint8)
+    if os.path.getsize(path) == 0:
+        return np.zeros(0, np.uint8)
+    return np.memmap(path, dtype=np.uint8, mode="r")
 
 
 def _device(a):
+    import warnings
+
     import torch
 
-    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    with warnings.catch_warnings():  # a read-only mapping is only read: copied to the device
+        warnings.simplefilter("ignore", UserWarning)
+        return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def _pinned_outputs(n: int, want_sa: bool, want_bwt: bool):
+    """Page-locked output buffers (the construction's merge writes them directly, with no separate
+    download), or None where page-locked memory is not available."""
+    import sadcs_b200 as sa
+
+    if n == 0:
+        return None, None, []
+    owned = []
+    try:
+        out_sa = out_bwt = None
+        if want_sa:
+            owned.append(sa.allocate_pinned(4 * n))
+            out_sa = owned[-1].view(np.uint32)
+        if want_bwt:
+            owned.append(sa.allocate_pinned(n))
+            out_bwt = owned[-1]
+        return out_sa, out_bwt, owned
+    except MemoryError:
+        for buffer in owned:
+            sa.free_pinned(buffer)
+        return None, None, []
 
 
 def _gpu_error(e) -> int:
@@ -63,7 +97,7 @@ def check_sa(text: np.ndarray, sa_array: np.ndarray):
     import sadcs_b200 as sa
 
     d_text = _device(text)
-    d_sa = _device(sa_array.astype(np.uint32))
+    d_sa = _device(np.ascontiguousarray(sa_array, dtype=np.uint32))
     return sa.check_suffix_array_device(d_text.data_ptr(), len(text), d_sa.data_ptr())
 
 
@@ -82,16 +116,22 @@ def cmd_build(a) -> int:
     text = _load(a.paths[0])
     n = len(text)
     stats = sa.Stats()
-    start = time.perf_counter()
+    out_sa, out_bwt, owned = _pinned_outputs(n, not a.bwt, a.bwt)
     try:
-        suffixes, bwt, primary = sa.build(text, want_sa=not a.bwt, want_bwt=a.bwt, stats=stats)
-    except sa.GpuError as e:
-        return _gpu_error(e)
-    seconds = time.perf_counter() - start
-    if a.bwt:
-        fileio.write_bwt(a.paths[1], bwt, primary)
-    else:
-        fileio.write_suffix_array(a.paths[1], suffixes)
+        start = time.perf_counter()
+        try:
+            suffixes, bwt, primary = sa.build(text, want_sa=not a.bwt, want_bwt=a.bwt, stats=stats, out_sa=out_sa,
+                                              out_bwt=out_bwt)
+        except sa.GpuError as e:
+            return _gpu_error(e)
+        seconds = time.perf_counter() - start
+        if a.bwt:
+            fileio.write_bwt(a.paths[1], bwt, primary)
+        else:
+            fileio.write_suffix_array(a.paths[1], suffixes)
+    finally:
+        for buffer in owned:
+            sa.free_pinned(buffer)
     print(f"{a.paths[0]} -> {a.paths[1]}: {n} bytes, GPU, {seconds:.3f}s ({_mbs(n, seconds):.1f} MB/s), peak device "
           f"memory {stats.device_bytes / MIB:.1f} MiB ({stats.device_bytes / max(n, 1):.2f} bytes per input byte)")
     return EXIT_OK
@@ -121,7 +161,7 @@ def cmd_check(a) -> int:
         print(f"{a.paths[1]}: BWT OK ({n} bytes, primary index {primary}, {seconds:.3f}s)")
         return EXIT_OK
     try:
-        sa_array = fileio.read_suffix_array(a.paths[1], n)
+        sa_array = fileio.read_suffix_array(a.paths[1], n, dtype=np.uint32)
     except ValueError:
         print(f"sadcs: cannot read '{a.paths[1]}' as a suffix array")
         return EXIT_ERROR

@@ -10,23 +10,53 @@
 """
 from __future__ import annotations
 
+import os
+
 import numpy as np
 
 INT32_LIMIT = (1 << 31) - 1025
+CHUNK = 1 << 24  # entries converted at a time for the 64-bit format (128 MiB of uint64)
 
 
-def write_suffix_array(path, sa: np.ndarray, n: int | None = None) -> None:
-    n = len(sa) if n is None else n
-    dtype = "<i4" if n <= INT32_LIMIT else "<u8"
-    np.ascontiguousarray(sa, dtype=dtype).tofile(path)
+def write_suffix_array(path, sa: np.ndarray, n: int | None = None, chunk: int = CHUNK) -> None:
+    """Writes the first n entries of sa. int32 entries are written from the array itself when it
+    holds 32-bit integers (no converted copy); the 64-bit extension converts chunk entries at a
+    time, so a 3 GiB text's suffix array never needs a 24 GiB uint64 copy."""
+    a = np.asarray(sa)
+    n = len(a) if n is None else n
+    a = a[:n]
+    if n <= INT32_LIMIT:
+        if a.dtype in (np.int32, np.uint32) and a.dtype.byteorder in "=<|" and a.flags.c_contiguous:
+            a.view("<i4").tofile(path)  # entries of a suffix array of n <= INT32_LIMIT are below 2^31
+        else:
+            np.ascontiguousarray(a, dtype="<i4").tofile(path)
+        return
+    with open(path, "wb") as f:
+        for start in range(0, n, chunk):
+            np.ascontiguousarray(a[start:start + chunk], dtype="<u8").tofile(f)
 
 
-def read_suffix_array(path, n: int) -> np.ndarray:
-    """The suffix array of a text of n bytes (int32 or, for the extension, uint64 entries)."""
-    size = np.memmap(path, dtype=np.uint8, mode="r").size if n else 0
+def read_suffix_array(path, n: int, dtype=None, chunk: int = CHUNK) -> np.ndarray:
+    """The suffix array of a text of n bytes (int32 or, for the extension, uint64 entries).
+
+    By default int32 entries come back as int32 (int64 past INT32_LIMIT) and uint64 ones as int64.
+    dtype=np.uint32 reads either format into one uint32 array (what the device checker takes), the
+    64-bit one chunk entries at a time; an entry that does not fit (a corrupt file) becomes
+    0xFFFFFFFF, which the checker reports as out of range."""
+    size = os.path.getsize(path) if n else 0
     if size == 4 * n:
-        return np.fromfile(path, dtype="<i4").astype(np.int64 if n > INT32_LIMIT else np.int32)
+        a = np.fromfile(path, dtype="<i4") if n else np.zeros(0, "<i4")
+        if dtype is not None and np.dtype(dtype) == np.uint32:
+            return a.view(np.uint32)
+        return a.astype(np.int64 if n > INT32_LIMIT else np.int32, copy=False)
     if size == 8 * n:
+        if dtype is not None and np.dtype(dtype) == np.uint32:
+            out = np.empty(n, np.uint32)
+            with open(path, "rb") as f:
+                for start in range(0, n, chunk):
+                    part = np.fromfile(f, dtype="<u8", count=min(chunk, n - start))
+                    out[start:start + len(part)] = np.minimum(part, 0xFFFFFFFF)
+            return out
         return np.fromfile(path, dtype="<u8").astype(np.int64)
     raise ValueError(f"{path}: {size} bytes is neither 4n nor 8n for n = {n}")
 
@@ -42,7 +72,7 @@ def write_bwt(path, bwt: np.ndarray, primary: int) -> None:
             f.write(np.int32(-1).tobytes())
             f.write(np.int64(n).tobytes())
             f.write(np.int64(primary).tobytes())
-        f.write(np.ascontiguousarray(bwt, dtype=np.uint8).tobytes())
+        np.ascontiguousarray(bwt, dtype=np.uint8).tofile(f)
 
 
 def read_bwt(path):
