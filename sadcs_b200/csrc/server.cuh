@@ -20,6 +20,8 @@
 #include <thread>
 #include <unordered_map>
 
+#include "server_policy.h"
+
 namespace {
 
 struct ServerRequest {
@@ -201,29 +203,17 @@ void serverWorker(sadcs_gpu_server* srv) {
             for (;;) {
                 if (srv->stopping && srv->queue.empty()) break;
                 if (!srv->queue.empty()) {
-                    // Take the head alone (large) or the queued small requests that fit one batch.
-                    std::vector<uint64_t> lengths;
-                    size_t take = 0, bytes = 0;
-                    for (ServerRequest* r : srv->queue) {
-                        const bool small = r->n <= srv->smallLimit;
-                        if (take == 0) {
-                            lengths.push_back(r->n);
-                            bytes += r->n;
-                            take = 1;
-                            if (!small) break;
-                            continue;
-                        }
-                        if (!small || bytes + r->n > srv->batchBytes || take >= srv->batchTexts) break;
-                        lengths.push_back(r->n);
-                        bytes += r->n;
-                        take++;
-                    }
+                    // Take the head alone (large) or the queued small requests that fit one batch
+                    // (server_policy.h).
+                    const size_t take = serverGroupSize(
+                        srv->queue.size(), [srv](size_t k) { return srv->queue[k]->n; }, srv->smallLimit,
+                        srv->batchBytes, srv->batchTexts);
+                    std::vector<uint64_t> lengths(take);
+                    for (size_t k = 0; k < take; k++) lengths[k] = srv->queue[k]->n;
                     Batch candidate;
                     planBatch(lengths.data(), static_cast<uint32_t>(lengths.size()), candidate);
                     const size_t need = footprintOf(candidate);
-                    // Admit when it fits beside the running ones; a request alone on an idle device
-                    // is always admitted (the budget check then is the allocation itself).
-                    if (need + srv->inUse <= srv->budget || srv->inUse == 0) {
+                    if (serverAdmits(need, srv->inUse, srv->budget)) {
                         for (size_t k = 0; k < take; k++) {
                             group.push_back(srv->queue.front());
                             srv->queue.pop_front();
