@@ -5,7 +5,8 @@ batch it admits is laid out from its own extent, and the construction refuses a 
 the slab. So every field of a batch's extent, and its layout's peak with or without the SA and BWT
 inside the slab, must stay within the bound's, for any texts of at most `capacity` bytes together
 and at most `texts` of them. Also checked: texts start on a cover period, in order, with prefix-sum
-sample and output bases, and the residue classes partition the positions. CPU only."""
+sample and output bases, the residue classes partition the positions, and the merge's top level
+fits one tile. CPU only."""
 import ctypes
 import shutil
 import subprocess
@@ -19,7 +20,7 @@ ROOT = HERE.parent
 SOURCE = HERE / "plan_harness.cu"
 BUILT = HERE / "_build" / "libplan_harness.so"
 CHECKS = {1: "planBatch refused", 2: "text not on a period", 3: "text length", 4: "texts out of order",
-          5: "sample or output base", 6: "totals", 7: "span", 8: "class partition",
+          5: "sample or output base", 6: "totals", 7: "span", 8: "class partition", 9: "top merge level over a tile",
           **{10 + f: f"extent field {name} over the bound" for f, name in enumerate(
               ["span", "slots", "live", "outputs", "largestClass", "splitterWords", "rows", "count"])},
           20: "layout peak over the bound's", 21: "layout peak over the context's slab"}
