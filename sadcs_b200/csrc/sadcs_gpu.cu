@@ -19,6 +19,8 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "alphabet.cuh"
 #include "bwt.cuh"
 #include "check.cuh"
@@ -57,6 +59,21 @@ constexpr int64_t kMemoryReserve = int64_t(256) << 20;          // gpusa.h:82
 constexpr int64_t kMaxInt32Text = int64_t(INT32_MAX) - 1024;    // src/cpu/dcsort.h:21
 constexpr int64_t kMaxText = (int64_t(1) << 32) - 256;
 constexpr uint32_t kMaxTexts = 1u << 20;
+
+// NVTX ranges of a construction's phases (upload, ranking, classes, merge) on the calling thread,
+// for profiler timelines and `ncu --nvtx --nvtx-include "sadcs merge/"`; without a tool attached
+// each call returns at once. The range open when the construction returns, on any path, is closed.
+class PhaseRange {
+public:
+    explicit PhaseRange(const char* name) { nvtxRangePushA(name); }
+    void next(const char* name) {
+        nvtxRangePop();
+        nvtxRangePushA(name);
+    }
+    ~PhaseRange() { nvtxRangePop(); }
+    PhaseRange(const PhaseRange&) = delete;
+    PhaseRange& operator=(const PhaseRange&) = delete;
+};
 
 size_t align256(size_t bytes) {
     return (bytes + 255) & ~size_t(255);
@@ -528,6 +545,7 @@ int construct(sadcs_gpu_context* c, const Batch& b, Io& io, cudaStream_t stream,
     texts.blockText = J > 1 ? dBlockText : nullptr;
 
     // Upload: one text straight into place; several through the ranking region, then placed.
+    PhaseRange phase("sadcs upload");
     auto start = std::chrono::steady_clock::now();
     const uint8_t* source = io.hostText ? io.hostText : io.deviceText;
     if (J == 1) {
@@ -575,6 +593,7 @@ int construct(sadcs_gpu_context* c, const Batch& b, Io& io, cudaStream_t stream,
     cudaEventRecord(c->events[0], stream);
 
     // The alphabet and the packed code stream.
+    phase.next("sadcs ranking");
     const uint64_t scanned = J == 1 ? b.end[0] : b.end[J - 1];
     if ((error = prepareAlphabet(text, scanned, b.span, reinterpret_cast<uint32_t*>(slab + L.alphabet),
                                  c->hostWords + c->hostWordCount - 256, reinterpret_cast<uint64_t*>(slab + L.packed),
@@ -616,6 +635,7 @@ int construct(sadcs_gpu_context* c, const Batch& b, Io& io, cudaStream_t stream,
     start = std::chrono::steady_clock::now();
 
     // Class lists.
+    phase.next("sadcs classes");
     uint32_t* lists = reinterpret_cast<uint32_t*>(slab + L.lists);
     uint32_t* classScratch = reinterpret_cast<uint32_t*>(slab + L.classScratch);
     uint64_t* const chains[2] = {reinterpret_cast<uint64_t*>(slab + L.chain0), reinterpret_cast<uint64_t*>(slab + L.chain1)};
@@ -635,6 +655,7 @@ int construct(sadcs_gpu_context* c, const Batch& b, Io& io, cudaStream_t stream,
     start = std::chrono::steady_clock::now();
 
     // Merge.
+    phase.next("sadcs merge");
     uint32_t* const* saPieces = io.saPieces ? reinterpret_cast<uint32_t* const*>(dPieces) : nullptr;
     uint8_t* const* bwtPieces = io.bwtPieces ? reinterpret_cast<uint8_t* const*>(dPieces + J) : nullptr;
     uint32_t* sa = saPieces ? nullptr
@@ -1229,6 +1250,7 @@ int sadcs_gpu_lcp(const uint8_t* d_text, int64_t n, const uint32_t* d_sa, uint32
         return SADCS_FAILED;
     }
     cudaStream_t st = static_cast<cudaStream_t>(stream);
+    PhaseRange phase("sadcs lcp");
     uint32_t* scratch = nullptr;
     cudaError_t error = cudaMallocAsync(&scratch, 4 * lcp::scratchWords(static_cast<uint64_t>(n)), st);
     if (error != cudaSuccess) return failed("cudaMallocAsync", error);
