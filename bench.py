@@ -1,11 +1,12 @@
 """bench.py - suffix array + BWT construction throughput on B200, and the reference CPU arm.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload natural256m|uniform8m|genome3g]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload genome3g|natural256m|natural64m|uniform8m]
     python bench.py --workload batch4096 | serve | lcp256m    batched, served, LCP array from text + SA
     python bench.py --impl reference ...       the reference's CPU variant on the host cores
     python bench.py --impl reference-gpu ...   the reference's own CUDA build on this GPU
 
 One step = one construction of the SA (uint32) and BWT of the workload's text, produced together.
+The default workload is the 3 GiB genome-like text (uint32 SA past the reference's int32 limit).
 ``value`` is device throughput with the text resident in HBM (CUDA events on the stream the library
 launches on, max over ranks); ``e2e`` is the same metric through the host C ABI (sadcs_gpu_build)
 from page-locked host memory, with the upload of the text and the download of SA and BWT inside
@@ -19,7 +20,13 @@ of the reference pipeline's named steps (sample ranking 12.375, class lists 11.7
 6). Peak = the measured HBM copy bandwidth in MEASURED_PEAKS.json (fallback 6650 GB/s).
 
 Multi-GPU: a single text does not shard, so N ranks build N independent replicas ("replicas",
-weak scaling); value = N * n / max-over-ranks time.
+weak scaling); value = N * n / max-over-ranks time. Without a launcher, --gpus N > 1 starts the N
+ranks itself (torch.distributed.run on this node).
+
+Beside the line's own figures: ``cpu_baseline`` (the reference's CPU build on a prefix sample, the
+same sample as the --impl reference arm) and, on one GPU, ``reference_gpu`` (the reference's own
+CUDA build on this GPU, on the largest prefix its int32 API takes, SA then BWT, next to this
+library's construction of the same prefix).
 """
 from __future__ import annotations
 
@@ -64,6 +71,26 @@ WORKLOADS = {
     "genome3g": ("3 GiB {A,C,G,T}: 2 GiB i.i.d. GC 0.41, then 1 GiB of mutated copies of 1 MiB segments "
                  "(1% substitutions, 0.1% indels of 1-10), seed 3", lambda W: W.genome_text(3 << 30, seed=3)),
 }
+# The first k bytes of a workload's text without generating all of it, where the generator allows.
+PREFIXES = {"genome3g": lambda W, k: W.genome_text(3 << 30, seed=3, prefix=k)}
+WORKLOAD_BYTES = {"natural256m": 256 << 20, "natural64m": 64 << 20, "uniform8m": 8 << 20, "genome3g": 3 << 30}
+DEFAULT_WORKLOAD = "genome3g"
+REFERENCE_INT32_LIMIT = (1 << 31) - 1025  # the reference's largest input (src/cpu/dcsort.h:21)
+
+
+def workload_prefix(name: str, k: int) -> np.ndarray:
+    from sadcs_b200 import workloads as W
+
+    if name in PREFIXES and k <= (WORKLOAD_BYTES[name] * 2) // 3:
+        return PREFIXES[name](W, k)
+    return np.ascontiguousarray(WORKLOADS[name][1](W)[:k])
+
+
+def workload_config(name: str, n: int, world: int) -> dict:
+    """The line's `config`, the same in this library's arm and the reference arm."""
+    return {"workload": name, "description": WORKLOADS[name][0], "text_bytes": n,
+            "outputs": "SA + BWT of the text", "l2": "inputs larger than L2 (text %d MiB)" % (n >> 20),
+            "parallelism": "replicas" if world > 1 else "single GPU"}
 
 
 def hbm_peak():
@@ -202,10 +229,12 @@ def batch_share(count_per_rank: int, world: int, rank: int) -> list[int]:
 
 # ---- CPU baseline (the reference's own CPU variant, or the oracle port) ----------------------------
 
-def cpu_baseline(text: np.ndarray, sample_bytes: int) -> dict:
+def cpu_baseline(sample: np.ndarray) -> dict:
+    """The reference's CPU build (or the oracle port) on a prefix sample of the workload's text:
+    SA then BWT, as the reference's CLI builds them."""
     import oracle
 
-    sample = np.ascontiguousarray(text[:sample_bytes])
+    sample = np.ascontiguousarray(sample)
     if oracle.ref_available():
         L = oracle.ref()
         cores = oracle.host_cores()
@@ -233,10 +262,9 @@ def run_reference(args, world, rank) -> None:
     import oracle
     from sadcs_b200 import workloads as W
 
-    desc, gen = WORKLOADS[args.workload]
-    text = gen(W)
-    n_sample = min(len(text), args.reference_sample_mib << 20)
-    sample = np.ascontiguousarray(text[:n_sample])
+    n = WORKLOAD_BYTES[args.workload]
+    n_sample = min(n, args.reference_sample_mib << 20)
+    sample = workload_prefix(args.workload, n_sample)
     if oracle.ref_available():
         L = oracle.ref()
         cores = oracle.host_cores()
@@ -265,84 +293,127 @@ def run_reference(args, world, rank) -> None:
     line = {"impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(mean * 1e3, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
-            "config": {"workload": args.workload, "description": desc, "text_bytes": int(len(text)),
-                       "sample_bytes": int(n_sample), "outputs": "SA + BWT (two reference CPU runs)"},
+            "config": workload_config(args.workload, n, 1),
             "cpu_baseline": {"value": round(value, 3), "unit": UNIT, "cores": cores, "kind": kind,
-                             "sample": f"first {n_sample / MIB:.0f} MiB of the workload text per step, SA then BWT, "
+                             "sample": f"first {n_sample / MIB:.0f} MiB of the workload text per step (of "
+                                       f"{n / MIB:.0f} MiB), SA then BWT (two runs), "
                                        f"{'reference CPU build (cover 128)' if kind == 'reference' else 'oracle port'}"},
             "e2e": {"value": round(value, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
-def run_reference_gpu(args, world, rank) -> None:
-    """--impl reference-gpu: the reference's own CUDA build (oracle/_ref/libsadcs_ref_gpu.so, its
-    gpusa.cu compiled unchanged for sm_100a) on this GPU, as its CLI's `bench --context --pinned`
-    measures it: page-locked host buffers, one context, gpuSuffixArray then gpuBwt per step (the
-    reference builds SA and BWT in two constructions), host to host. Rank 0 only."""
-    if rank != 0:
-        return
-    import ctypes
-
+def time_reference_gpu(text: np.ndarray, steps: int, warmup: int) -> dict:
+    """The reference's own CUDA build (oracle/_ref/libsadcs_ref_gpu.so: its gpusa.cu compiled
+    unchanged for sm_100a) on this GPU, as its CLI's `bench --context --pinned` measures it:
+    page-locked host buffers, one context, gpuSuffixArray then gpuBwt per step (the reference
+    builds SA and BWT in two constructions), host to host; device time from its own GpuStats.
+    Returns the figures, or {"unavailable": why}."""
     import oracle
-    from sadcs_b200 import workloads as W
 
-    desc, gen = WORKLOADS[args.workload]
-    base = {"impl": "reference-gpu", "metric": METRIC, "unit": UNIT}
     if not oracle.ref_gpu_available():
-        print(json.dumps({**base, "unavailable": "oracle/_ref/libsadcs_ref_gpu.so not built (make -C oracle ref-gpu "
-                                                 "needs the reference sources)"}), flush=True)
-        return
-    text = gen(W)
+        return {"unavailable": "oracle/_ref/libsadcs_ref_gpu.so not built (make -C oracle ref-gpu needs the "
+                               "reference sources)"}
     n = int(len(text))
-    if n > (1 << 31) - 1025:
-        print(json.dumps({**base, "unavailable": "the reference's GPU API takes int32 sizes up to 2^31 - 1025 bytes"}),
-              flush=True)
-        return
+    if n > REFERENCE_INT32_LIMIT:
+        return {"unavailable": "the reference's GPU API takes int32 sizes up to 2^31 - 1025 bytes"}
     try:
         ctx = oracle.RefGpuContext(n)
     except RuntimeError as e:
-        print(json.dumps({**base, "unavailable": str(e)}), flush=True)
-        return
+        return {"unavailable": str(e)}
     h_text = oracle.ref_gpu_pinned(n)
     h_sa = oracle.ref_gpu_pinned(4 * n)
     h_bwt = oracle.ref_gpu_pinned(n)
     try:
+        if h_text is None or h_sa is None or h_bwt is None:
+            return {"unavailable": "the reference's gpuAllocatePinned failed"}
         h_text[:] = text
         sa_view = h_sa.view(np.int32)
+        sa_ms, bwt_ms = [], []
 
         def step():
             _, sa_dev = ctx.suffix_array(h_text, out=sa_view)
             _, primary, bwt_dev = ctx.bwt(h_text, out=h_bwt)
-            return sa_dev + bwt_dev, primary
+            return sa_dev, bwt_dev
 
-        for _ in range(max(args.warmup, 0)):
+        for _ in range(max(warmup, 0)):
             step()
-        host, device = [], []
-        for _ in range(args.steps):
+        host = []
+        for _ in range(steps):
             t0 = time.perf_counter()
-            dev, primary = step()
+            a, b = step()
             host.append(time.perf_counter() - t0)
-            device.append(dev)
+            sa_ms.append(a * 1e3)
+            bwt_ms.append(b * 1e3)
         mean_host = sum(host) / len(host)
-        mean_dev = sum(device) / len(device)
-        value = n / MIB / mean_host
-        print(json.dumps({
-            **base, "value": round(value, 3), "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": round(mean_host * 1e3, 3), "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "u8", "data": "synthetic",
-            "config": {"workload": args.workload, "description": desc, "text_bytes": n,
-                       "outputs": "SA (int32) by gpuSuffixArray, then BWT by gpuBwt (two constructions)",
-                       "cover": "mod 32 (the reference's GPU cover)", "build": "reference gpusa.cu, nvcc 12.9, sm_100a"},
-            "device_value": round(n / MIB / mean_dev, 3),
-            "device_ms_per_step": round(mean_dev * 1e3, 3),
-            "e2e": {"value": round(value, 3), "unit": UNIT, "h2d_bytes_per_step": 2 * n, "d2h_bytes_per_step": 5 * n,
-                    "api": "gpuSuffixArray + gpuBwt with a context and page-locked buffers"},
-        }), flush=True)
+        mean_dev = (sum(sa_ms) + sum(bwt_ms)) / len(host)
+        return {"value": round(n / MIB / mean_host, 3), "unit": UNIT, "ms_per_step": round(mean_host * 1e3, 3),
+                "device_value": round(n / MIB / (mean_dev / 1e3), 3), "device_ms_per_step": round(mean_dev, 3),
+                "device_ms_sa": round(sum(sa_ms) / len(sa_ms), 3), "device_ms_bwt": round(sum(bwt_ms) / len(bwt_ms), 3),
+                "text_bytes": n, "steps": steps, "warmup": warmup,
+                "outputs": "SA (int32) by gpuSuffixArray, then BWT by gpuBwt (two constructions)",
+                "cover": "mod 32 (the reference's GPU cover)", "build": "reference gpusa.cu, nvcc 12.9, sm_100a",
+                "h2d_bytes_per_step": 2 * n, "d2h_bytes_per_step": 5 * n}
     finally:
         ctx.close()
         for a in (h_text, h_sa, h_bwt):
             if a is not None:
                 oracle.ref_gpu_free_pinned(a)
+
+
+def run_reference_gpu(args, world, rank) -> None:
+    """--impl reference-gpu: time_reference_gpu on the workload's text (or its largest prefix the
+    reference takes). Rank 0 only."""
+    if rank != 0:
+        return
+    n = min(WORKLOAD_BYTES[args.workload], REFERENCE_INT32_LIMIT)
+    record = time_reference_gpu(workload_prefix(args.workload, n), args.steps, args.warmup)
+    base = {"impl": "reference-gpu", "metric": METRIC, "unit": UNIT}
+    if "unavailable" in record:
+        print(json.dumps({**base, **record}), flush=True)
+        return
+    print(json.dumps({
+        **base, "value": record["value"], "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": record["ms_per_step"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u8", "data": "synthetic", "config": workload_config(args.workload, n, 1),
+        "device_value": record["device_value"], "device_ms_per_step": record["device_ms_per_step"],
+        "e2e": {"value": record["value"], "unit": UNIT, "h2d_bytes_per_step": record["h2d_bytes_per_step"],
+                "d2h_bytes_per_step": record["d2h_bytes_per_step"],
+                "api": "gpuSuffixArray + gpuBwt with a context and page-locked buffers"},
+    }), flush=True)
+
+
+def reference_gpu_record(args, d_text, ctx, text: np.ndarray, stream) -> dict:
+    """The kernel bar: the reference's CUDA build and this library on the same input (the
+    workload's text, or its largest prefix the reference's int32 API takes), on this GPU. Ours is
+    one construction of SA + BWT, device time by CUDA events; the reference's is its SA and its
+    BWT construction, device time by its own stats."""
+    import torch
+
+    import sadcs_b200 as sa
+
+    n = min(len(text), REFERENCE_INT32_LIMIT)
+    record = time_reference_gpu(np.ascontiguousarray(text[:n]), args.reference_gpu_steps, 1)
+    if "unavailable" in record:
+        return record
+    d_sa = torch.empty(n, dtype=torch.int32, device=d_text.device)
+    d_bwt = torch.empty(n, dtype=torch.uint8, device=d_text.device)
+    times = []
+    for i in range(1 + args.reference_gpu_steps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        sa.build_device(d_text.data_ptr(), n, d_sa.data_ptr(), d_bwt.data_ptr(), context=ctx,
+                        stream=stream.cuda_stream)
+        b.record(stream)
+        torch.cuda.synchronize()
+        if i > 0:
+            times.append(a.elapsed_time(b))
+    ours_ms = sum(times) / len(times)
+    record["ours_same_input"] = {"device_ms_per_step": round(ours_ms, 3),
+                                 "device_value": round(n / MIB / (ours_ms / 1e3), 3),
+                                 "outputs": "SA (uint32) + BWT from one construction"}
+    record["device_speedup"] = round(record["device_ms_per_step"] / ours_ms, 3)
+    record["input"] = "the workload text" if n == len(text) else f"the first {n} bytes of the workload text"
+    return record
 
 
 # ---- our arm --------------------------------------------------------------------------------------
@@ -426,11 +497,9 @@ def run_ours(args, world, rank, local) -> None:
     line = {"metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms_max, 3), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u8", "data": "synthetic",
-            "config": {"workload": args.workload, "description": desc, "text_bytes": n,
-                       "outputs": "SA (uint32) + BWT from one construction", "cover": "mod 32 (7 of 32)",
-                       "l2": "inputs larger than L2 (text %d MiB; working set %.1f GB)" % (
-                           n >> 20, sa.required_bytes(n) / 1e9),
-                       "parallelism": "replicas" if world > 1 else "single GPU"},
+            "config": workload_config(args.workload, n, world),
+            "construction": {"outputs": "SA (uint32) + BWT from one construction", "cover": "mod 32 (7 of 32)",
+                             "working_set_gb": round(sa.required_bytes(n) / 1e9, 2)},
             "roofline": roofline,
             "pipeline_roofline": {"bound": "hbm", "achieved": round(pipe_gbs, 1), "peak": peak, "unit": "GB/s",
                                   "frac": round(pipe_gbs / peak, 4),
@@ -442,7 +511,9 @@ def run_ours(args, world, rank, local) -> None:
     if e2e:
         line["e2e"] = e2e
     if world == 1 and args.cpu_sample_mib > 0:
-        line["cpu_baseline"] = cpu_baseline(text, args.cpu_sample_mib << 20)
+        line["cpu_baseline"] = cpu_baseline(text[:args.cpu_sample_mib << 20])
+    if world == 1 and args.reference_gpu_steps > 0:
+        line["reference_gpu"] = reference_gpu_record(args, d_text, ctx, text, stream)
     print(json.dumps(line), flush=True)
 
 
@@ -838,13 +909,26 @@ def run_serve(args, world, rank, local) -> None:
         }), flush=True)
 
 
+def launch_ranks(gpus: int) -> None:
+    """--gpus N > 1 without a launcher: starts this same command as N ranks on this node
+    (torch.distributed.run, rendezvous on 127.0.0.1) and exits with its status."""
+    import socket
+
+    with socket.socket() as probe:
+        probe.bind(("127.0.0.1", 0))
+        port = probe.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={gpus}",
+           "--master-addr", "127.0.0.1", "--master-port", str(port), str(Path(__file__).resolve()), *sys.argv[1:]]
+    sys.exit(subprocess.call(cmd))
+
+
 def main() -> None:
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference", "reference-gpu"], default="ours")
-    p.add_argument("--workload", choices=sorted(WORKLOADS) + ["batch4096", "serve", "lcp256m"], default="natural256m")
+    p.add_argument("--workload", choices=sorted(WORKLOADS) + ["batch4096", "serve", "lcp256m"], default=DEFAULT_WORKLOAD)
     p.add_argument("--batch-count", type=int, default=4096)
     p.add_argument("--plain-sample", type=int, default=64)
     p.add_argument("--serve-loads", default="50,200,800")
@@ -854,9 +938,17 @@ def main() -> None:
     p.add_argument("--cpu-sample-mib", type=int, default=64)
     p.add_argument("--reference-sample-mib", type=int, default=64)
     p.add_argument("--e2e-steps", type=int, default=3)
+    p.add_argument("--reference-gpu-steps", type=int, default=2,
+                   help="steps of the reference CUDA build in the line's reference_gpu record (0: none)")
     p.add_argument("--no-e2e", dest="e2e", action="store_false")
     p.add_argument("--no-verify", dest="verify", action="store_false")
     args = p.parse_args()
+    if "WORLD_SIZE" not in os.environ and args.gpus > 1:
+        launch_ranks(args.gpus)  # does not return
+    if int(os.environ.get("WORLD_SIZE", "1")) != args.gpus:
+        print(f"bench.py: --gpus {args.gpus} but the launcher started {os.environ.get('WORLD_SIZE')} ranks",
+              file=sys.stderr)
+        sys.exit(2)
     if args.impl == "reference-gpu":
         world, rank, _ = rank_env()
         run_reference_gpu(args, world, rank)

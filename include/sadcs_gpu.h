@@ -178,7 +178,9 @@ int sadcs_gpu_check_suffix_array(const uint8_t* d_text, int64_t n, const uint32_
  * up to SADCS_GPU_STATIC_CHECK_MAX entries, plus three result words). n above that limit is rejected
  * with SADCS_FAILED and a message naming the limit; nothing is launched.
  * The first call on each device looks up the array's address (cudaGetSymbolAddress), which may load
- * the library's device code: make that first call before capturing any stream.
+ * the library's device code: make that first call before capturing any stream. The address is kept
+ * for the life of the process, so do not call this entry point again on a device after
+ * cudaDeviceReset (the reset unloads the device code, and the array may come back elsewhere).
  * Initial values: the array keeps whatever the last call left; each call sets what must start
  * known before its kernels run: its three result words to all ones and the first n words of the
  * inverse suffix array to zero.
@@ -223,6 +225,20 @@ void sadcs_gpu_server_destroy(sadcs_gpu_server* server);
  * device memory. */
 int sadcs_gpu_check_bwt(const uint8_t* d_text, int64_t n, const uint8_t* d_bwt, int64_t primary, int64_t* bad_index,
                         void* stream);
+
+/* checkSuffixArray in fast mode (src/common/checker.h:24, checker.cpp:53-109) with host buffers, for
+ * n up to 2^32 - 256 (uint32 entries; the reference's int32 array views the same bytes): text (n
+ * bytes, no padding needed) and sa (n entries) are copied to the device and checked there by
+ * sadcs_gpu_check_suffix_array. *bad_index and *reason as there (CheckResult's index and reason).
+ * Uses 9n bytes of temporary device memory. Returns SADCS_OK whenever the check ran. */
+int sadcs_gpu_check_suffix_array_host(const uint8_t* text, int64_t n, const uint32_t* sa, int64_t* bad_index,
+                                      const char** reason);
+
+/* checkBwt (src/common/checker.h:29, checker.cpp:196-245) with host buffers: text and bwt (n bytes
+ * each) and primary, checked on the device by sadcs_gpu_check_bwt. *bad_index = -1 if the BWT
+ * inverts to the text, else the first text position where it does not (0 if it does not invert).
+ * Uses about 27n bytes of temporary device memory. */
+int sadcs_gpu_check_bwt_host(const uint8_t* text, int64_t n, const uint8_t* bwt, int64_t primary, int64_t* bad_index);
 
 /* No counterpart: the inverse BWT (unbwt) on the device: d_text (n bytes) from d_bwt and primary.
  * Returns SADCS_FAILED if d_bwt is not a valid BWT. */

@@ -164,6 +164,11 @@ def lib() -> ctypes.CDLL:
         L.sadcs_gpu_check_suffix_array_static.restype = ctypes.c_int
         L.sadcs_gpu_check_suffix_array_static.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, _i64p,
                                                           ctypes.POINTER(ctypes.c_char_p), ctypes.c_void_p]
+        L.sadcs_gpu_check_suffix_array_host.restype = ctypes.c_int
+        L.sadcs_gpu_check_suffix_array_host.argtypes = [_u8p, ctypes.c_int64, _u32p, _i64p,
+                                                        ctypes.POINTER(ctypes.c_char_p)]
+        L.sadcs_gpu_check_bwt_host.restype = ctypes.c_int
+        L.sadcs_gpu_check_bwt_host.argtypes = [_u8p, ctypes.c_int64, _u8p, ctypes.c_int64, _i64p]
         L.sadcs_gpu_lcp.restype = ctypes.c_int
         L.sadcs_gpu_lcp.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
         _lib = L
@@ -398,6 +403,33 @@ def check_bwt_device(d_text: int, n: int, d_bwt: int, primary: int, stream: int 
     index = ctypes.c_int64(-1)
     _check(lib().sadcs_gpu_check_bwt(ctypes.c_void_p(d_text), int(n), ctypes.c_void_p(d_bwt), int(primary),
                                      ctypes.byref(index), ctypes.c_void_p(stream) if stream else None))
+    return index.value < 0, int(index.value)
+
+
+def check_suffix_array(text, suffixes: np.ndarray):
+    """checkSuffixArray in fast mode (src/common/checker.h:24) on host arrays, run on the device
+    (sadcs_gpu_check_suffix_array_host): (ok, first failing SA index, reason)."""
+    t = _as_text(text)
+    s = np.ascontiguousarray(suffixes)
+    if s.dtype not in (np.uint32, np.int32) or len(s) != len(t):
+        raise ValueError("the suffix array must hold one 32-bit entry per text byte")
+    index = ctypes.c_int64(-1)
+    reason = ctypes.c_char_p()
+    _check(lib().sadcs_gpu_check_suffix_array_host(t.ctypes.data_as(_u8p), len(t), s.ctypes.data_as(_u32p),
+                                                   ctypes.byref(index), ctypes.byref(reason)))
+    return index.value < 0, int(index.value), reason.value.decode() if reason.value else None
+
+
+def check_bwt(text, bwt_bytes: np.ndarray, primary: int):
+    """checkBwt (src/common/checker.h:29) on host arrays, run on the device
+    (sadcs_gpu_check_bwt_host): (ok, first text position where the inverse differs)."""
+    t = _as_text(text)
+    b = _as_text(bwt_bytes)
+    if len(b) != len(t):
+        raise ValueError("the BWT must have as many bytes as the text")
+    index = ctypes.c_int64(-1)
+    _check(lib().sadcs_gpu_check_bwt_host(t.ctypes.data_as(_u8p), len(t), b.ctypes.data_as(_u8p), int(primary),
+                                          ctypes.byref(index)))
     return index.value < 0, int(index.value)
 
 

@@ -2,10 +2,10 @@
 
 The reference's commands and flags (src/cli/main.cpp:73-154), its output lines and exit codes
 (0 ok, 1 error); the construction always runs on the GPU (cover mod 32; --cover and --threads are
-accepted and do not apply, as for the reference's --gpu). Checks run on the GPU too
-(sadcs_gpu_check_suffix_array / sadcs_gpu_check_bwt). Texts past the reference's int32 limit use the
-64-bit file formats of sadcs_b200.fileio. The reference's own CLI also links unchanged against
-libsadcs_gpu.so through include/gpusa.h.
+accepted and do not apply, as for the reference's --gpu). Checks run on the GPU too, from host
+buffers (sadcs_gpu_check_suffix_array_host / sadcs_gpu_check_bwt_host). Texts past the reference's
+int32 limit use the 64-bit file formats of sadcs_b200.fileio. The reference's own CLI also links
+unchanged against libsadcs_gpu.so through include/gpusa.h.
 
   sadcs build|-b [--bwt] <in> <out> [--gpu]
   sadcs check|-c [--bwt] <in> <in.sa|in.bwt>
@@ -51,16 +51,6 @@ def _load(path) -> np.ndarray:
     return np.memmap(path, dtype=np.uint8, mode="r")
 
 
-def _device(a):
-    import warnings
-
-    import torch
-
-    with warnings.catch_warnings():  # a read-only mapping is only read: copied to the device
-        warnings.simplefilter("ignore", UserWarning)
-        return torch.from_numpy(np.ascontiguousarray(a)).cuda()
-
-
 def _pinned_outputs(n: int, want_sa: bool, want_bwt: bool):
     """Page-locked output buffers (the construction's merge writes them directly, with no separate
     download), or None where page-locked memory is not available."""
@@ -94,17 +84,17 @@ def _gpu_error(e) -> int:
 
 
 def check_sa(text: np.ndarray, sa_array: np.ndarray):
+    """(ok, first failing SA index, reason): the reference checker's fast mode, on the device."""
     import sadcs_b200 as sa
 
-    d_text = _device(text)
-    d_sa = _device(np.ascontiguousarray(sa_array, dtype=np.uint32))
-    return sa.check_suffix_array_device(d_text.data_ptr(), len(text), d_sa.data_ptr())
+    return sa.check_suffix_array(text, np.ascontiguousarray(sa_array, dtype=np.uint32))
 
 
 def check_bwt(text: np.ndarray, bwt: np.ndarray, primary: int):
+    """(ok, first text position where the inverse differs): the reference's BWT check, on the device."""
     import sadcs_b200 as sa
 
-    return sa.check_bwt_device(_device(text).data_ptr(), len(text), _device(bwt).data_ptr(), primary)
+    return sa.check_bwt(text, bwt, primary)
 
 
 def cmd_build(a) -> int:

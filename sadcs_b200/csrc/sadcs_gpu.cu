@@ -1242,6 +1242,87 @@ int sadcs_gpu_check_bwt(const uint8_t* d_text, int64_t n, const uint8_t* d_bwt, 
     return status;
 }
 
+}  // extern "C"
+
+namespace {
+
+// Device copies of a host check's inputs, on a stream of the check's own; the destructor frees
+// them and the stream once the check's work on it is done.
+struct HostCheckInputs {
+    cudaStream_t stream = nullptr;
+    void* first = nullptr;
+    void* second = nullptr;
+
+    cudaError_t upload(const void* a, size_t aBytes, const void* b, size_t bBytes) {
+        cudaError_t error;
+        if ((error = cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking)) != cudaSuccess) {
+            stream = nullptr;
+            return error;
+        }
+        if ((error = cudaMallocAsync(&first, aBytes, stream)) != cudaSuccess) return error;
+        if ((error = cudaMallocAsync(&second, bBytes, stream)) != cudaSuccess) return error;
+        if ((error = cudaMemcpyAsync(first, a, aBytes, cudaMemcpyHostToDevice, stream)) != cudaSuccess) return error;
+        return cudaMemcpyAsync(second, b, bBytes, cudaMemcpyHostToDevice, stream);
+    }
+    ~HostCheckInputs() {
+        if (!stream) return;
+        if (first) cudaFreeAsync(first, stream);
+        if (second) cudaFreeAsync(second, stream);
+        cudaStreamSynchronize(stream);
+        cudaStreamDestroy(stream);
+    }
+};
+
+}  // namespace
+
+extern "C" {
+
+int sadcs_gpu_check_suffix_array_host(const uint8_t* text, int64_t n, const uint32_t* sa, int64_t* bad_index,
+                                      const char** reason) {
+    tLastError[0] = '\0';
+    if (bad_index) *bad_index = -1;
+    if (reason) *reason = nullptr;
+    if (n <= 0) return SADCS_OK;
+    if (n > kMaxText) {
+        setError("text of %lld bytes exceeds the limit of %lld", static_cast<long long>(n), static_cast<long long>(kMaxText));
+        return SADCS_FAILED;
+    }
+    if (!text || !sa) {
+        setError("text or suffix array is null");
+        return SADCS_FAILED;
+    }
+    HostCheckInputs in;
+    if (const cudaError_t error = in.upload(text, static_cast<size_t>(n), sa, 4 * static_cast<size_t>(n));
+        error != cudaSuccess) {
+        return failed("uploading the check's inputs", error);
+    }
+    return sadcs_gpu_check_suffix_array(static_cast<const uint8_t*>(in.first), n,
+                                        static_cast<const uint32_t*>(in.second), bad_index, reason, in.stream);
+}
+
+int sadcs_gpu_check_bwt_host(const uint8_t* text, int64_t n, const uint8_t* bwt, int64_t primary, int64_t* bad_index) {
+    tLastError[0] = '\0';
+    if (bad_index) *bad_index = -1;
+    if (n <= 0 || primary < 1 || primary > n) {  // decided without the device, as the device check does
+        return sadcs_gpu_check_bwt(nullptr, n, nullptr, primary, bad_index, nullptr);
+    }
+    if (n > kMaxText) {
+        setError("text of %lld bytes exceeds the limit of %lld", static_cast<long long>(n), static_cast<long long>(kMaxText));
+        return SADCS_FAILED;
+    }
+    if (!text || !bwt) {
+        setError("text or BWT is null");
+        return SADCS_FAILED;
+    }
+    HostCheckInputs in;
+    if (const cudaError_t error = in.upload(text, static_cast<size_t>(n), bwt, static_cast<size_t>(n));
+        error != cudaSuccess) {
+        return failed("uploading the check's inputs", error);
+    }
+    return sadcs_gpu_check_bwt(static_cast<const uint8_t*>(in.first), n, static_cast<const uint8_t*>(in.second),
+                               primary, bad_index, in.stream);
+}
+
 int sadcs_gpu_lcp(const uint8_t* d_text, int64_t n, const uint32_t* d_sa, uint32_t* d_lcp, void* stream) {
     tLastError[0] = '\0';
     if (n <= 0) return SADCS_OK;

@@ -141,23 +141,31 @@ def natural_text(n: int = 256 << 20, seed: int = 2, vocabulary: int = 50_000, zi
 _DNA = np.frombuffer(b"ACGT", np.uint8)
 
 
-def _iid_dna(rng: np.random.Generator, n: int, gc: float = 0.41) -> np.ndarray:
-    out = np.empty(n, np.uint8)
+def _iid_dna(rng: np.random.Generator, n: int, gc: float = 0.41, out: np.ndarray | None = None) -> np.ndarray:
+    out = np.empty(n, np.uint8) if out is None else out
     cdf = np.cumsum([(1 - gc) / 2, gc / 2, gc / 2, (1 - gc) / 2])
-    chunk = 1 << 26
+    chunk = 1 << 20  # small temporaries are reused by the allocator instead of faulted in afresh
+    c = cdf.astype(np.float32)
     for s in range(0, n, chunk):
         u = rng.random(min(chunk, n - s), dtype=np.float32)
-        out[s:s + len(u)] = _DNA[np.searchsorted(cdf.astype(np.float32), u, side="right").clip(0, 3)]
+        # letter index = how many of the first three cdf entries are <= u (u < 1 = the last entry)
+        index = (u >= c[0]).view(np.uint8) + (u >= c[1]).view(np.uint8) + (u >= c[2]).view(np.uint8)
+        out[s:s + len(u)] = _DNA[index]
     return out
 
 
 def genome_text(n: int = 3 << 30, seed: int = 3, segment: int = 1 << 20, substitution: float = 0.01,
-                indel: float = 0.001) -> np.ndarray:
-    """2/3 i.i.d. DNA (GC 0.41), then mutated copies of random ``segment``-long pieces of it."""
+                indel: float = 0.001, prefix: int | None = None) -> np.ndarray:
+    """2/3 i.i.d. DNA (GC 0.41), then mutated copies of random ``segment``-long pieces of it.
+
+    ``prefix`` <= 2n/3: only the first ``prefix`` bytes of that text (the i.i.d. part is one
+    sequential stream, so they come out the same without generating the rest)."""
     rng = np.random.default_rng(seed)
     base_len = (n * 2) // 3
+    if prefix is not None and prefix <= base_len:
+        return _iid_dna(rng, prefix)
     out = np.empty(n, np.uint8)
-    out[:base_len] = _iid_dna(rng, base_len)
+    _iid_dna(rng, base_len, out=out[:base_len])
     filled = base_len
     while filled < n:
         start = int(rng.integers(0, max(1, base_len - segment)))

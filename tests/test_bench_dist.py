@@ -103,3 +103,31 @@ def test_reference_arm_unavailable_lines(workload):
     assert proc.returncode == 0, proc.stderr
     line = json.loads(proc.stdout.strip().splitlines()[-1])
     assert line["impl"] == "reference" and "unavailable" in line
+
+
+def test_gpus_flag_must_match_the_launcher():
+    """--gpus N with a launcher that started another number of ranks is refused (exit 2), rather
+    than running fewer replicas than asked and reporting them as N."""
+    env = dict(os.environ, RANK="0", LOCAL_RANK="0", WORLD_SIZE="1")
+    proc = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--impl", "reference", "--gpus", "2",
+                           "--steps", "1", "--warmup", "0"], env=env, capture_output=True, text=True, timeout=120)
+    assert proc.returncode == 2
+    assert "--gpus 2" in proc.stderr
+
+
+def test_gpus_flag_without_a_launcher_starts_the_ranks():
+    """--gpus 2 with no launcher starts two ranks itself; the reference arm's rank 0 prints the one
+    line and rank 1 exits without work."""
+    env = {k: v for k, v in os.environ.items() if k not in ("WORLD_SIZE", "RANK", "LOCAL_RANK")}
+    proc = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--impl", "reference", "--gpus", "2",
+                           "--workload", "uniform8m", "--steps", "1", "--warmup", "0", "--reference-sample-mib", "1"],
+                          env=env, capture_output=True, text=True, timeout=300)
+    assert proc.returncode == 0, proc.stderr[-2000:]
+    lines = [json.loads(x) for x in proc.stdout.splitlines() if x.startswith("{")]
+    assert len(lines) == 1 and lines[0]["impl"] == "reference"
+    sys.path.insert(0, str(ROOT))
+    import bench
+
+    # the reference arm's config is the one this library's arm reports for the same workload
+    assert lines[0]["config"] == bench.workload_config("uniform8m", 8 << 20, 1)
+    assert lines[0]["cpu_baseline"]["sample"].startswith("first 1 MiB")

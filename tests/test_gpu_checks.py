@@ -21,7 +21,8 @@ def test_suffix_array_check_accepts_and_rejects():
     text = W.random_text(rng, 3000, 3)
     good = oracle.naive_sa(text)
     d_text = _device(text)
-    ok, index, _ = sa.check_suffix_array_device(d_text.data_ptr(), len(text), _device(good).data_ptr())
+    d_good = _device(good)  # held until the check returns: a freed block could be handed out again
+    ok, index, _ = sa.check_suffix_array_device(d_text.data_ptr(), len(text), d_good.data_ptr())
     assert ok and index == -1
     mutations = {
         "swapped neighbours": lambda s: s.__setitem__(slice(1000, 1002), s[1000:1002][::-1].copy()),
@@ -32,7 +33,8 @@ def test_suffix_array_check_accepts_and_rejects():
     for name, mutate in mutations.items():
         bad = good.copy()
         mutate(bad)
-        ok, index, reason = sa.check_suffix_array_device(d_text.data_ptr(), len(text), _device(bad).data_ptr())
+        d_bad = _device(bad)
+        ok, index, reason = sa.check_suffix_array_device(d_text.data_ptr(), len(text), d_bad.data_ptr())
         assert not ok and index >= 0 and reason, name
         if name == "duplicate entry":
             # the smallest index of any repeated entry, whatever order the scatter ran in
@@ -61,7 +63,8 @@ def test_bwt_check_and_inverse():
     for name, b, p in (("changed character", changed, primary),
                        ("primary off by one", bwt, primary + 1 if primary < 3000 else primary - 1),
                        ("primary 0", bwt, 0)):
-        ok, _ = sa.check_bwt_device(d_text.data_ptr(), len(text), _device(b).data_ptr(), p)
+        d_b = _device(b)
+        ok, _ = sa.check_bwt_device(d_text.data_ptr(), len(text), d_b.data_ptr(), p)
         assert not ok, name
 
 
@@ -95,3 +98,29 @@ def test_inverse_bwt_across_chunks_past_2g():
     d_bwt[n - 7] ^= 2  # one changed byte in the last chunk
     ok, _ = sa.check_bwt_device(d_text.data_ptr(), n, d_bwt.data_ptr(), primary)
     assert not ok
+
+
+def test_host_buffer_checks_agree_with_the_device_checks():
+    """sadcs_gpu_check_suffix_array_host / sadcs_gpu_check_bwt_host (checkSuffixArray and checkBwt
+    with host buffers) give the verdicts of the device-buffer entry points."""
+    text = W.natural_text(1 << 18, seed=31)
+    good = oracle.doubling_sa(text).astype(np.uint32)
+    bwt, primary = oracle.bwt_from_sa(text, good)
+    assert sa.check_suffix_array(text, good) == (True, -1, None)
+    assert sa.check_bwt(text, bwt, primary) == (True, -1)
+    d_text = _device(text)
+    for name, mutate in (("swap", lambda s: s.__setitem__([7, 8], s[[8, 7]])),
+                         ("duplicate", lambda s: s.__setitem__(100, s[5000])),
+                         ("out of range", lambda s: s.__setitem__(3, len(s) + 3))):
+        bad = good.copy()
+        mutate(bad)
+        d_bad = _device(bad)
+        expected = sa.check_suffix_array_device(d_text.data_ptr(), len(text), d_bad.data_ptr())
+        assert sa.check_suffix_array(text, bad) == expected and not expected[0], name
+    changed = bwt.copy()
+    changed[len(text) // 2] ^= 0x20
+    d_changed = _device(changed)
+    expected = sa.check_bwt_device(d_text.data_ptr(), len(text), d_changed.data_ptr(), primary)
+    assert sa.check_bwt(text, changed, primary) == expected and not expected[0]
+    assert sa.check_bwt(text, bwt, 0) == (False, 0)
+    assert sa.check_bwt(text[:0], bwt[:0], 0) == (True, -1)

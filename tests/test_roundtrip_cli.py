@@ -51,3 +51,25 @@ def test_empty_input(tmp_path):
     assert cli.main(["build", "--bwt", str(source), str(tmp_path / "empty.bwt")]) == 0
     bwt, primary = fileio.read_bwt(tmp_path / "empty.bwt")
     assert len(bwt) == 0 and primary == 0
+
+
+def test_test_and_selftest_commands(tmp_path):
+    """`test` and `test --bwt` build each file and check it against the file itself (text and BWT
+    of the same length, the case where a check that freed its device copy of the text too early
+    compared the BWT with itself); `selftest` runs the adversarial families through both checks."""
+    W.natural_text(300_000, seed=53).tofile(tmp_path / "natural")
+    W.random_text(W.SplitMix(54), 50_000, 4).tofile(tmp_path / "dna")
+    W.run_text(4096).tofile(tmp_path / "run")
+    assert cli.main(["test", str(tmp_path)]) == 0
+    assert cli.main(["test", "--bwt", str(tmp_path)]) == 0
+    assert cli.main(["selftest"]) == 0
+
+
+def test_check_rejects_a_bwt_that_is_not_the_texts(tmp_path):
+    text = W.natural_text(200_000, seed=55)
+    other = W.natural_text(200_000, seed=56)
+    source = tmp_path / "in.txt"
+    text.tofile(source)
+    eb, ep = oracle.bwt_from_sa(other, oracle.doubling_sa(other))
+    fileio.write_bwt(tmp_path / "other.bwt", eb, ep)
+    assert cli.main(["check", "--bwt", str(source), str(tmp_path / "other.bwt")]) == 1

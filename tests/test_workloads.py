@@ -65,6 +65,15 @@ def test_genome_text_shape():
     assert np.isin(fresh, known).mean() < 0.01
 
 
+def test_genome_prefix_is_the_texts_start():
+    """The prefix path (used to sample the 3 GiB text for the CPU baseline without generating all
+    of it) gives the same bytes as the whole text's start, across generator chunk boundaries."""
+    n = 6 << 20
+    text = W.genome_text(n, seed=3, segment=1 << 16)
+    for k in (1, 12345, 1 << 20, (1 << 20) + 7, 2 * n // 3):
+        assert np.array_equal(W.genome_text(n, seed=3, segment=1 << 16, prefix=k), text[:k])
+
+
 def test_batch_shapes():
     """4096 lengths log-uniform in [1 KiB, 4 MiB] (mean about 0.48 MiB, about 1.9 GiB in all); texts by
     index mod 3 over DNA, 20 amino acids and uniform bytes."""

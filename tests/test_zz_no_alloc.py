@@ -33,6 +33,27 @@ def _cases(text):
             "out of range": out}
 
 
+def _memory_state():
+    """What an allocation would change: the device's free memory, torch's allocator counters and the
+    used and reserved bytes of the device's current stream-ordered memory pool."""
+    import torch
+
+    torch.cuda.synchronize()
+    state = {"free": torch.cuda.mem_get_info()[0], "torch_allocated": torch.cuda.memory_allocated(),
+             "torch_reserved": torch.cuda.memory_reserved()}
+    from cuda.bindings import runtime as rt
+
+    error, device = rt.cudaGetDevice()
+    assert error == rt.cudaError_t.cudaSuccess
+    error, pool = rt.cudaDeviceGetMemPool(device)
+    assert error == rt.cudaError_t.cudaSuccess
+    for name in ("cudaMemPoolAttrUsedMemCurrent", "cudaMemPoolAttrReservedMemCurrent"):
+        error, value = rt.cudaMemPoolGetAttribute(pool, getattr(rt.cudaMemPoolAttr, name))
+        assert error == rt.cudaError_t.cudaSuccess
+        state[name] = int(value)
+    return state
+
+
 def _compare(text):
     d_text = _device(text)
     for name, s in _cases(text).items():
@@ -66,3 +87,16 @@ def test_rejects_inputs_beyond_its_scratch():
     # the allocating entry point takes the same input
     ok, index, reason = sa.check_suffix_array_device(d_text.data_ptr(), n, d_sa.data_ptr())
     assert not ok
+
+
+def test_a_call_allocates_nothing():
+    """After one call (the first call on a device looks up the scratch array's address), further
+    calls leave the device's free memory, torch's allocator and the stream-ordered pool unchanged."""
+    text = W.natural_text(1 << 16, seed=14)
+    d_text = _device(text)
+    d_sa = _device(oracle.doubling_sa(text).astype(np.uint32))
+    assert sa.check_suffix_array_static_device(d_text.data_ptr(), len(text), d_sa.data_ptr()) == (True, -1, None)
+    before = _memory_state()
+    for _ in range(2):
+        assert sa.check_suffix_array_static_device(d_text.data_ptr(), len(text), d_sa.data_ptr()) == (True, -1, None)
+    assert _memory_state() == before
