@@ -70,10 +70,14 @@ WORKLOADS = {
     "uniform8m": ("8 MiB i.i.d. uniform bytes, seed 1", lambda W: W.uniform_bytes(8 << 20, seed=1)),
     "genome3g": ("3 GiB {A,C,G,T}: 2 GiB i.i.d. GC 0.41, then 1 GiB of mutated copies of 1 MiB segments "
                  "(1% substitutions, 0.1% indels of 1-10), seed 3", lambda W: W.genome_text(3 << 30, seed=3)),
+    "genome256m": ("256 MiB {A,C,G,T} built as genome3g at 1/12 the size (the profiling case: its 235 MB rank "
+                   "array exceeds L2, with about 4.5 GB on the device)",
+                   lambda W: W.genome_text(256 << 20, seed=3)),
 }
 # The first k bytes of a workload's text without generating all of it, where the generator allows.
 PREFIXES = {"genome3g": lambda W, k: W.genome_text(3 << 30, seed=3, prefix=k)}
-WORKLOAD_BYTES = {"natural256m": 256 << 20, "natural64m": 64 << 20, "uniform8m": 8 << 20, "genome3g": 3 << 30}
+WORKLOAD_BYTES = {"natural256m": 256 << 20, "natural64m": 64 << 20, "uniform8m": 8 << 20, "genome3g": 3 << 30,
+                  "genome256m": 256 << 20}
 DEFAULT_WORKLOAD = "genome3g"
 REFERENCE_INT32_LIMIT = (1 << 31) - 1025  # the reference's largest input (src/cpu/dcsort.h:21)
 

@@ -36,8 +36,11 @@ def _cases(text):
 def _memory_state():
     """What an allocation would change: the device's free memory, torch's allocator counters and the
     used and reserved bytes of the device's current stream-ordered memory pool."""
+    import gc
+
     import torch
 
+    gc.collect()  # tensors of earlier tests freed now, not between two readings
     torch.cuda.synchronize()
     state = {"free": torch.cuda.mem_get_info()[0], "torch_allocated": torch.cuda.memory_allocated(),
              "torch_reserved": torch.cuda.memory_reserved()}
