@@ -168,55 +168,66 @@ __device__ __forceinline__ int listOfElement(const uint32_t* seg, uint32_t e) {
     return l;
 }
 
-// Thread 0 of a tile: its window in every list (t.win, t.seg), the number of elements before the
-// windows (t.base), the window indices of the tile's two splitters (t.loIdx, t.hiIdx; kNoList for
-// the ends of the level) and whether the window set fits (t.bad otherwise, never by construction).
+// Warp 0 of a tile (all 32 lanes): its window in every list (t.win, t.seg; lane b plans list b),
+// the number of elements before the windows (t.base), the window indices of the tile's two
+// splitters (t.loIdx, t.hiIdx; kNoList for the ends of the level) and whether the window set fits
+// (t.bad otherwise, never by construction).
 __device__ __forceinline__ void planTileWindows(const MergeArgs& a, MergeTileInfo& t) {
     const uint32_t* st = a.level.start;
-    uint32_t w[kClasses], e[kClasses];
+    const uint32_t b = threadIdx.x & 31;
+    uint32_t w = 0, e = 0;
     uint32_t loList = kNoList, hiList = kNoList;
     if (!a.rowsIn) {
-        for (int b = 0; b < kClasses; b++) {
-            w[b] = 0;
-            e[b] = st[b + 1] - st[b];
-        }
+        if (b < kClasses) e = st[b + 1] - st[b];
     } else {
-        const MergeRow lo = a.rowsIn[blockIdx.x];
-        const MergeRow hi = a.rowsIn[blockIdx.x + 1];
-        loList = lo.list;
-        hiList = hi.list;
-        for (int b = 0; b < kClasses; b++) {
+        const MergeRow* lo = a.rowsIn + blockIdx.x;
+        const MergeRow* hi = lo + 1;
+        loList = lo->list;
+        hiList = hi->list;
+        if (b < kClasses) {
             const uint32_t len = st[b + 1] - st[b];
-            if (lo.list == kNoList) {
-                w[b] = 0;
-            } else if (static_cast<uint32_t>(b) == lo.list) {
-                w[b] = lo.c[b] * kMergeG;
+            const uint32_t cLo = lo->c[b], cHi = hi->c[b];
+            if (loList == kNoList) {
+                w = 0;
+            } else if (b == loList) {
+                w = cLo * kMergeG;
             } else {
-                w[b] = lo.c[b] == 0 ? 0 : (lo.c[b] - 1) * kMergeG + 1;
+                w = cLo == 0 ? 0 : (cLo - 1) * kMergeG + 1;
             }
-            if (hi.list == kNoList) {
-                e[b] = len;
-            } else if (static_cast<uint32_t>(b) == hi.list) {
-                e[b] = hi.c[b] * kMergeG + 1;
+            if (hiList == kNoList) {
+                e = len;
+            } else if (b == hiList) {
+                e = cHi * kMergeG + 1;
             } else {
-                e[b] = min(len, hi.c[b] * kMergeG);
+                e = min(len, cHi * kMergeG);
             }
-            w[b] = min(w[b], len);
-            e[b] = max(min(e[b], len), w[b]);
+            w = min(w, len);
+            e = max(min(e, len), w);
         }
     }
-    uint32_t base = 0;
-    t.seg[0] = 0;
-    for (int b = 0; b < kClasses; b++) {
-        t.win[b] = w[b];
-        t.seg[b + 1] = t.seg[b] + (e[b] - w[b]);
-        base += w[b];
+    // seg[b + 1] = the window lengths of lists 0..b (inclusive scan over the lanes)
+    uint32_t seg = e - w;
+#pragma unroll
+    for (int d = 1; d < 8; d <<= 1) {
+        const uint32_t v = __shfl_up_sync(0xffffffffu, seg, d);
+        if (b >= static_cast<uint32_t>(d)) seg += v;
     }
-    t.base = base;
-    t.size = t.seg[kClasses];
-    t.loIdx = loList == kNoList ? kNoList : t.seg[loList];
-    t.hiIdx = hiList == kNoList ? kNoList : t.seg[hiList + 1] - 1;
-    t.bad = t.size > kMergeCap;
+    const uint32_t base = __reduce_add_sync(0xffffffffu, w);
+    const uint32_t size = __shfl_sync(0xffffffffu, seg, kClasses - 1);
+    const uint32_t loStart = loList == kNoList || loList == 0 ? 0u : __shfl_sync(0xffffffffu, seg, (loList - 1) & 31);
+    const uint32_t hiEnd = hiList == kNoList ? 0u : __shfl_sync(0xffffffffu, seg, hiList & 31);
+    if (b < kClasses) {
+        t.win[b] = w;
+        t.seg[b + 1] = seg;
+    }
+    if (b == 0) {
+        t.seg[0] = 0;
+        t.base = base;
+        t.size = size;
+        t.loIdx = loList == kNoList ? kNoList : loStart;
+        t.hiIdx = hiList == kNoList ? kNoList : hiEnd - 1;
+        t.bad = size > kMergeCap;
+    }
 }
 
 // S_{L+1}: every G-th element of each list of level L.

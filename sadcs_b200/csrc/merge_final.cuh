@@ -130,10 +130,21 @@ __device__ __forceinline__ bool headLess(const FinalTile<W, kMulti>& s, const Fi
     return __ldg(s.ranks + pack(i + k)) < __ldg(s.ranks + pack(j + k));
 }
 
+// Record index at position x of a level's source order: src[x], or x itself for the first level,
+// whose source is the windows in list order (kIdentity: src is not read).
+template <bool kIdentity>
+__device__ __forceinline__ uint32_t sourceAt(const uint16_t* src, uint32_t x) {
+    if constexpr (kIdentity) {
+        return x;
+    } else {
+        return src[x];
+    }
+}
+
 // One tree level: the merges m (A = [mb[3m], mb[3m + 1]), B = [mb[3m + 1], mb[3m + 2]) of src,
 // written to dst from mb[3m]), which together cover [0, size); mb is in shared memory. Thread t
 // writes outputs [t * chunk, (t + 1) * chunk).
-template <int W, bool kMulti>
+template <int W, bool kMulti, bool kIdentity>
 __device__ __forceinline__ void finalLevel(const FinalTile<W, kMulti>& s, const uint16_t* src, uint16_t* dst,
                                            const uint32_t* mb, int merges, uint32_t size, uint32_t n,
                                            uint32_t bits) {
@@ -150,49 +161,75 @@ __device__ __forceinline__ void finalLevel(const FinalTile<W, kMulti>& s, const 
         uint32_t lo = d > lenB ? d - lenB : 0, hi = min(d, lenA);
         while (lo < hi) {
             const uint32_t mid = (lo + hi) >> 1;
-            if (headLess(s, loadHead(s, src[a0 + mid]), loadHead(s, src[a1 + d - 1 - mid]), n, bits)) {
+            if (headLess(s, loadHead(s, sourceAt<kIdentity>(src, a0 + mid)),
+                         loadHead(s, sourceAt<kIdentity>(src, a1 + d - 1 - mid)), n, bits)) {
                 lo = mid + 1;
             } else {
                 hi = mid;
             }
         }
         uint32_t i = lo, j = d - lo;
-        FinalHead ha{}, hb{};
-        if (i < lenA) ha = loadHead(s, src[a0 + i]);
-        if (j < lenB) hb = loadHead(s, src[a1 + j]);
+        // Both heads in registers; a step takes one side and loads that side's next record (the
+        // merge's first record when the side is used up: in range, and never compared again), so
+        // the lanes of a warp do not diverge on which side they took.
+        FinalHead ha = loadHead(s, sourceAt<kIdentity>(src, i < lenA ? a0 + i : a0));
+        FinalHead hb = loadHead(s, sourceAt<kIdentity>(src, j < lenB ? a1 + j : a0));
         for (; d < stop; d++) {
-            if (j == lenB || (i < lenA && headLess(s, ha, hb, n, bits))) {
-                dst[a0 + d] = static_cast<uint16_t>(ha.idx);
-                i++;
-                if (i < lenA) ha = loadHead(s, src[a0 + i]);
+            const bool takeA = j == lenB || (i < lenA && headLess(s, ha, hb, n, bits));
+            dst[a0 + d] = static_cast<uint16_t>(takeA ? ha.idx : hb.idx);
+            i += takeA ? 1u : 0u;
+            j += takeA ? 0u : 1u;
+            const uint32_t x = takeA ? (i < lenA ? a0 + i : a0) : (j < lenB ? a1 + j : a0);
+            const FinalHead h = loadHead(s, sourceAt<kIdentity>(src, x));
+            if (takeA) {
+                ha = h;
             } else {
-                dst[a0 + d] = static_cast<uint16_t>(hb.idx);
-                j++;
-                if (j < lenB) hb = loadHead(s, src[a1 + j]);
+                hb = h;
             }
         }
         at = a0 + stop;
     }
 }
 
+// Tiles resident per SM the register budget is set for. One code word per record leaves room in
+// shared memory for 5 tiles of 384 threads, but at the 32 registers that allows the kernel spills:
+// 4 tiles without spills were 3% faster on the 3 GiB genome-like text (168.3 against 173.2 ms);
+// wider records fill shared memory at 4 (tuning).
+#ifndef SADCS_MERGE_TILES_W1
+#define SADCS_MERGE_TILES_W1 4
+#endif
+template <int W>
+constexpr int mergeTilesPerSm() {
+    return W == 1 ? SADCS_MERGE_TILES_W1 : 4;
+}
+
 // kFinal: the last level, writing the SA and the BWT; otherwise an upper level, writing the rows
 // (every R-th element of the merged order with its per-list counts) that bound the tiles below.
 template <int W, bool kMulti, bool kFinal>
-__global__ void __launch_bounds__(kMergeThreads) mergeTree(MergeArgs a) {
+__global__ void __launch_bounds__(kMergeThreads, mergeTilesPerSm<W>()) mergeTree(MergeArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     FinalTile<W, kMulti> s;
     s.carve(smem, a.ranks);
     __shared__ MergeTileInfo t;
     __shared__ uint32_t sLo, sHi;
     __shared__ uint32_t bounds[3 * 7];  // the tree's merges: 4 + 2 + 1 triples of window offsets
-    if (threadIdx.x == 0) {
+    if (threadIdx.x < 32) {
         planTileWindows(a, t);
-        sLo = 0;
-        sHi = t.size;
-        // (0,1) (2,3) (4,5) (6,-), then (01,23) (45,6), then (0123,456): indices into t.seg
+        __syncwarp();
+        // (0,1) (2,3) (4,5) (6,-), then (01,23) (45,6), then (0123,456): indices into t.seg, 3 bits
+        // each (a register constant: a table indexed by the lane would live in local memory)
         constexpr uint8_t kTree[21] = {0, 1, 2, 2, 3, 4, 4, 5, 6, 6, 7, 7, 0, 2, 4, 4, 6, 7, 0, 4, 7};
-        for (int i = 0; i < 21; i++) bounds[i] = t.seg[kTree[i]];
-        if (t.bad && a.error) atomicExch(a.error, 1u);
+        constexpr uint64_t kTreePacked = [] {
+            uint64_t v = 0;
+            for (int i = 0; i < 21; i++) v |= static_cast<uint64_t>(kTree[i]) << (3 * i);
+            return v;
+        }();
+        if (threadIdx.x < 21) bounds[threadIdx.x] = t.seg[(kTreePacked >> (3 * threadIdx.x)) & 7];
+        if (threadIdx.x == 0) {
+            sLo = 0;
+            sHi = t.size;
+            if (t.bad && a.error) atomicExch(a.error, 1u);
+        }
     }
     __syncthreads();
     if (t.bad) return;
@@ -218,15 +255,18 @@ __global__ void __launch_bounds__(kMergeThreads) mergeTree(MergeArgs a) {
             p[j] = a.level.lists[st[l] + t.win[l] + (e - t.seg[l])];
         }
     }
-    uint32_t ends[kItems];  // the end of each position's text (one load chain per item, all in flight)
+    // The end of each position's text (several texts: one load chain per item, all in flight).
+    uint32_t ends[kMulti ? kItems : 1];
+    if constexpr (kMulti) {
 #pragma unroll
-    for (int j = 0; j < kItems; j++) ends[j] = threadIdx.x + j * kMergeThreads < size ? a.texts.endOf(p[j]) : 0;
+        for (int j = 0; j < kItems; j++) ends[j] = threadIdx.x + j * kMergeThreads < size ? a.texts.endOf(p[j]) : 0;
+    }
 #pragma unroll
     for (int j = 0; j < kItems; j++) {
         const uint32_t e = threadIdx.x + j * kMergeThreads;
         if (e < size) {
             uint32_t q = p[j];
-            const uint32_t qEnd = ends[j];
+            const uint32_t qEnd = kMulti ? ends[j] : a.texts.oneEnd;
             if (q >= qEnd) {  // cannot happen for valid class lists; never read out of range
                 atomicExch(a.error, 3u);
                 q = 0;
@@ -234,7 +274,6 @@ __global__ void __launch_bounds__(kMergeThreads) mergeTree(MergeArgs a) {
             p[j] = q;
             s.pos[e] = q;
             if constexpr (kMulti) s.end[e] = q < qEnd ? qEnd : a.texts.endOf(0);
-            s.idxA[e] = static_cast<uint16_t>(e);
             const uint64_t* src = a.texts.packed + ((static_cast<uint64_t>(q) * bits) >> 6);
 #pragma unroll
             for (int w = 0; w < W; w++) cpAsync8(&s.words[w * kMergeCap + e], src + w);
@@ -276,11 +315,11 @@ __global__ void __launch_bounds__(kMergeThreads) mergeTree(MergeArgs a) {
     __syncthreads();
 
     // The merge tree.
-    finalLevel(s, s.idxA, s.idxB, bounds, 4, size, n, bits);
+    finalLevel<W, kMulti, true>(s, nullptr, s.idxB, bounds, 4, size, n, bits);
     __syncthreads();
-    finalLevel(s, s.idxB, s.idxA, bounds + 12, 2, size, n, bits);
+    finalLevel<W, kMulti, false>(s, s.idxB, s.idxA, bounds + 12, 2, size, n, bits);
     __syncthreads();
-    finalLevel(s, s.idxA, s.idxB, bounds + 18, 1, size, n, bits);
+    finalLevel<W, kMulti, false>(s, s.idxA, s.idxB, bounds + 18, 1, size, n, bits);
     __syncthreads();
     const uint16_t* order = s.idxB;
 
