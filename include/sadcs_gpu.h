@@ -253,6 +253,16 @@ int sadcs_gpu_inverse_bwt(const uint8_t* d_bwt, int64_t n, int64_t primary, uint
  * unspecified d_lcp, never a read outside the buffers. */
 int sadcs_gpu_lcp(const uint8_t* d_text, int64_t n, const uint32_t* d_sa, uint32_t* d_lcp, void* stream);
 
+/* No counterpart: a test of the failure path of the radix passes' bounded wait (the decoupled
+ * look-back, which every construction's sorts use). Runs one radix pass on a stream of its own in
+ * which the only block waits on a predecessor tile that is never taken, so that nothing ever
+ * publishes the status it waits for; after limit_cycles SM cycles (1 to 4e9) of waiting the block
+ * gives up as a construction's pass would: it sets the pass's error word and stores nothing, and the
+ * kernel returns. *error_word gets the error word. Returns SADCS_FAILED with the message of the
+ * time-out when that happened (the expected outcome), SADCS_OK if the pass did not wait, and
+ * SADCS_FAILED with a CUDA error's message otherwise. Uses about 100 KB of temporary device memory. */
+int sadcs_gpu_test_lookback_timeout(int64_t limit_cycles, uint32_t* error_word);
+
 /* No counterpart: the capacity (bytes of text) of a context. */
 int64_t sadcs_gpu_context_capacity(const sadcs_gpu_context* context);
 

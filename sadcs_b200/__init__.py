@@ -169,6 +169,8 @@ def lib() -> ctypes.CDLL:
                                                         ctypes.POINTER(ctypes.c_char_p)]
         L.sadcs_gpu_check_bwt_host.restype = ctypes.c_int
         L.sadcs_gpu_check_bwt_host.argtypes = [_u8p, ctypes.c_int64, _u8p, ctypes.c_int64, _i64p]
+        L.sadcs_gpu_test_lookback_timeout.restype = ctypes.c_int
+        L.sadcs_gpu_test_lookback_timeout.argtypes = [ctypes.c_int64, _u32p]
         L.sadcs_gpu_lcp.restype = ctypes.c_int
         L.sadcs_gpu_lcp.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
         _lib = L
@@ -444,6 +446,14 @@ def lcp_device(d_text: int, n: int, d_sa: int, d_lcp: int, stream: int | None = 
     longest common prefix of suffixes d_sa[r - 1] and d_sa[r] (n uint32 entries; d_lcp may be d_sa)."""
     _check(lib().sadcs_gpu_lcp(ctypes.c_void_p(d_text), int(n), ctypes.c_void_p(d_sa), ctypes.c_void_p(d_lcp),
                                ctypes.c_void_p(stream) if stream else None))
+
+
+def test_lookback_timeout(limit_cycles: int):
+    """The radix look-back's time-out made to happen (sadcs_gpu_test_lookback_timeout): one pass
+    whose only block waits on a status nothing publishes. Returns (status, error word, message)."""
+    word = ctypes.c_uint32(0)
+    status = lib().sadcs_gpu_test_lookback_timeout(int(limit_cycles), ctypes.byref(word))
+    return GpuStatus(status), int(word.value), last_error()
 
 
 def allocate_pinned(nbytes: int) -> np.ndarray:

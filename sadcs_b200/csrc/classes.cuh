@@ -100,17 +100,71 @@ inline uint32_t* classErrorWord(uint32_t* scratch, uint32_t texts) {
     return radixErrorWord(classRadixScratch(scratch, texts));
 }
 
-// Class 0: the live sample positions in rank order, the ranks in [lo, hi) of them. The writes land
-// at random places of the list, so the caller covers the ranks in slices of the list (kRankSlice).
-__global__ void classScatterSample(const uint32_t* __restrict__ ranks, uint32_t slots, uint32_t lo, uint32_t hi,
-                                   TextSet texts, uint32_t* __restrict__ list) {
-    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= slots) return;
-    const uint32_t r = __ldcs(ranks + t);  // streamed: evicted first, so the list's slice stays
-    if (r < lo || r >= hi) return;
-    const uint32_t p = samplePosition(t);
-    if (p >= texts.endOf(p)) return;  // past the end, or between texts
-    list[r] = p;
+// Class 0: the live sample positions in rank order, list[rank] = position. The ranks of the live
+// samples are a permutation of [0, live), so the slice of ranks [k << shift, (k + 1) << shift)
+// holds exactly 2^shift samples (the last slice the rest). Two steps, so that no write lands at a
+// random place of the whole list: classPartitionSample streams the rank array once and writes each
+// live sample's (rank, position) pair into its rank's slice of a pair array (in any order inside
+// the slice; one run per slice and block); classScatterPairs then walks the pairs slice by slice,
+// and each slice's writes stay within the list's L2-sized slice.
+constexpr uint32_t kSampleSliceShift = 23;  // 8M ranks = 32 MB of the list per slice
+constexpr uint32_t kMaxSampleSlices = 128;
+constexpr int kPartitionThreads = 256;
+constexpr int kPartitionItems = 8;
+
+// The slice width (as a shift) for `live` samples: at least 8M ranks, at most kMaxSampleSlices slices.
+inline uint32_t sampleSliceShift(uint64_t live) {
+    uint32_t shift = kSampleSliceShift;
+    while ((live >> shift) >= kMaxSampleSlices) shift++;
+    return shift;
+}
+
+// fill[k] (zeroed by the caller) counts the pairs placed in slice k so far.
+__global__ void __launch_bounds__(kPartitionThreads) classPartitionSample(const uint32_t* __restrict__ ranks,
+                                                                         uint32_t slots, uint32_t live,
+                                                                         uint32_t shift, TextSet texts,
+                                                                         uint32_t* __restrict__ fill,
+                                                                         uint64_t* __restrict__ pairs) {
+    __shared__ uint32_t count[kMaxSampleSlices];
+    __shared__ uint32_t base[kMaxSampleSlices];
+    for (uint32_t i = threadIdx.x; i < kMaxSampleSlices; i += kPartitionThreads) count[i] = 0;
+    __syncthreads();
+    uint32_t r[kPartitionItems], p[kPartitionItems], local[kPartitionItems];
+    const uint64_t first = static_cast<uint64_t>(blockIdx.x) * kPartitionThreads * kPartitionItems + threadIdx.x;
+#pragma unroll
+    for (int j = 0; j < kPartitionItems; j++) {
+        const uint64_t t = first + static_cast<uint64_t>(j) * kPartitionThreads;
+        r[j] = 0xFFFFFFFFu;
+        if (t < slots) {
+            const uint32_t rank = __ldcs(ranks + t);  // streamed: read once
+            const uint32_t q = samplePosition(static_cast<uint32_t>(t));
+            if (q < texts.endOf(q) && rank < live) {  // a live sample (not past the end or between texts)
+                r[j] = rank;
+                p[j] = q;
+                local[j] = atomicAdd(&count[rank >> shift], 1u);
+            }
+        }
+    }
+    __syncthreads();
+    for (uint32_t k = threadIdx.x; k < kMaxSampleSlices; k += kPartitionThreads) {
+        if (count[k]) base[k] = atomicAdd(fill + k, count[k]);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < kPartitionItems; j++) {
+        if (r[j] == 0xFFFFFFFFu) continue;
+        const uint32_t k = r[j] >> shift;
+        const uint64_t at = (static_cast<uint64_t>(k) << shift) + base[k] + local[j];
+        if (at < live) pairs[at] = (static_cast<uint64_t>(r[j]) << 32) | p[j];  // always, for a permutation
+    }
+}
+
+__global__ void classScatterPairs(const uint64_t* __restrict__ pairs, uint32_t live, uint32_t* __restrict__ list) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= live) return;
+    const uint64_t v = __ldcs(pairs + i);
+    const uint32_t r = static_cast<uint32_t>(v >> 32);
+    if (r < live) list[r] = static_cast<uint32_t>(v);
 }
 
 // Codes of the 8 characters before p: byte i holds the code of T[p - 1 - i] (0 before position 0),
@@ -230,14 +284,15 @@ inline cudaError_t sortClasses(uint32_t total, const TextSet& texts, const uint3
                                uint64_t* const chains[2], cudaStream_t stream) {
     const uint32_t J = tables.texts;
     const uint32_t live = plan.start[1];
-    // Each slice reads every rank once: past kMaxRankSlices slices one plain pass costs less.
-    const uint32_t slice = ceilDiv(live, kRankSlice) <= kMaxRankSlices ? kRankSlice : live;
-    for (uint32_t lo = 0; lo < live; lo += slice) {
-        const uint32_t hi = live - lo > slice ? lo + slice : live;
-        SADCS_TRY(launch(classScatterSample, (slots + 255) / 256, 256, 0, stream, ranks, slots, lo, hi, texts, lists));
-    }
     uint32_t* hist = scratch;  // [kClasses][J][256]
     const RadixScratch radix(classRadixScratch(scratch, J), 0);
+    // Class 0 through the pair array (chain buffer 0, free until pass 1) and the slice counters
+    // (the radix scratch's digit-base words, unused by the class passes).
+    uint32_t* fill = radix.digitBase;
+    SADCS_TRY(cudaMemsetAsync(fill, 0, kMaxSampleSlices * sizeof(uint32_t), stream));
+    SADCS_TRY(launch(classPartitionSample, ceilDiv(slots, kPartitionThreads * kPartitionItems), kPartitionThreads, 0,
+                     stream, ranks, slots, live, sampleSliceShift(live), texts, fill, chains[0]));
+    SADCS_TRY(launch(classScatterPairs, ceilDiv(live, 256), 256, 0, stream, chains[0], live, lists));
     SADCS_TRY(cudaMemsetAsync(hist, 0, static_cast<size_t>(kClasses) * J * 256 * 4, stream));
     SADCS_TRY(cudaMemsetAsync(radix.control, 0, 8, stream));
     const uint32_t blocks = std::min<uint32_t>(ceilDiv(total + 7ull, 256 * 8 * 8), 148 * 8);

@@ -177,18 +177,6 @@ __host__ __device__ __forceinline__ uint32_t ceilDiv(uint64_t a, uint64_t b) {
 // a multiple of 32 so every position has the same residue modulo the cover period in its text and
 // in the concatenation; the bytes between texts are zero. blockText[p / 32] is the text whose range
 // contains or precedes block p / 32. With one text, blockText is null and its end is oneEnd.
-// Entries per slice of a scatter of 4-byte words to random places of a large array (the sample by
-// rank): each launch writes only the entries of one slice of the array, 24M = 96 MB by default,
-// so that most of the slice stays in L2 while the writes land (a write to a sector that is not
-// there costs a DRAM read of it). At 256 MiB of text the class phase took 5.19 ms with 24M slices
-// (3), 5.25 with 12M (5), 5.55 with 8M, 6.13 unsliced. Every slice reads the whole source, so at
-// most kMaxRankSlices of them (tuning).
-#ifndef SADCS_SCATTER_SLICE_M
-#define SADCS_SCATTER_SLICE_M 24
-#endif
-constexpr uint32_t kRankSlice = static_cast<uint32_t>(SADCS_SCATTER_SLICE_M) << 20;
-constexpr uint32_t kMaxRankSlices = 4;
-
 struct TextSet {
     const uint32_t* blockText;
     const uint32_t* start;

@@ -63,9 +63,11 @@ struct FinalTile {
 };
 
 // The fields of a record a comparison reads first, kept in registers while the merge walk holds
-// the record.
+// the record: its first code word, and with several texts its position and text end (the words
+// are masked to the shorter suffix). With one text the position is read only when the first 31
+// characters tie.
 struct FinalHead {
-    uint32_t idx, pos, rot, end;  // rot: coverRotation(pos); end: several texts only
+    uint32_t idx, pos, end;  // pos, end: several texts only
     uint64_t w0;
 };
 
@@ -73,9 +75,8 @@ template <int W, bool kMulti>
 __device__ __forceinline__ FinalHead loadHead(const FinalTile<W, kMulti>& s, uint32_t x) {
     FinalHead h;
     h.idx = x;
-    h.pos = s.pos[x];
-    h.rot = coverRotation(h.pos);
     h.w0 = s.words[x];
+    h.pos = kMulti ? s.pos[x] : 0;
     h.end = kMulti ? s.end[x] : 0;
     return h;
 }
@@ -93,9 +94,7 @@ __device__ __forceinline__ bool headLess(const FinalTile<W, kMulti>& s, const Fi
     if constexpr (kMulti) {
         if (a.end != b.end) return a.end < b.end;  // different texts: text order
         n = a.end;
-    }
-    const uint32_t i = a.pos, j = b.pos;
-    if constexpr (kMulti) {
+        const uint32_t i = a.pos, j = b.pos;
         const uint32_t lim = min(n - i, n - j) * bits;  // bits of the shorter suffix
         uint64_t x = a.w0, y = b.w0;
         if (lim < 64) {
@@ -124,7 +123,8 @@ __device__ __forceinline__ bool headLess(const FinalTile<W, kMulti>& s, const Fi
             if (x != y) return x < y;
         }
     }
-    const uint32_t k = tieOffset(a.rot, b.rot);
+    const uint32_t i = kMulti ? a.pos : s.pos[a.idx], j = kMulti ? b.pos : s.pos[b.idx];
+    const uint32_t k = tieOffset(coverRotation(i), coverRotation(j));
     if (k > min(n - i, n - j) || i + k == n || j + k == n) return i > j;  // one is a prefix of the other
     // rare (2-3% of the comparisons on natural and DNA-like text): the ranks come from global memory
     return __ldg(s.ranks + pack(i + k)) < __ldg(s.ranks + pack(j + k));

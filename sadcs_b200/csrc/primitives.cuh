@@ -178,7 +178,8 @@ constexpr uint32_t kStatusPrefix = 2u << 30;
 constexpr uint32_t kStatusValue = (1u << 30) - 1;
 constexpr uint32_t kMaxSortCount = kStatusValue;
 // The look-back gives up after this many SM cycles of waiting (2 s at the B200's 1965 MHz, longer at
-// lower clocks): far above any real wait. The SM's own cycle counter is monotonic for the thread
+// lower clocks): far above any real wait. (A kernel parameter, so that a test can make it give up
+// quickly on a predecessor that never publishes.) The SM's own cycle counter is monotonic for the thread
 // that reads it; a global-timer reading can jump when its two halves are read across a carry.
 constexpr long long kLookbackLimitCycles = 4000000000ll;
 
@@ -225,12 +226,18 @@ struct ManySegments {
 // element takes part, its key and digit (load), and later its value (value, called again for the
 // same elements only, so that values are not held in registers through ranking and look-back).
 // Storers write keys (when kKeys) and values at output positions.
+// Tiles resident per SM the register budget is set for (tuning).
+#ifndef SADCS_SORT_TILES
+#define SADCS_SORT_TILES 3
+#endif
+
 template <class Key, class Loader, class Storer, class Segments = OneSegment>
-__global__ void __launch_bounds__(kSortThreads, 3) radixOnesweep(Loader ld, Storer st, Segments segs,
+__global__ void __launch_bounds__(kSortThreads, SADCS_SORT_TILES) radixOnesweep(Loader ld, Storer st, Segments segs,
                                                                  const uint32_t* __restrict__ digitBase,
                                                                  uint32_t* __restrict__ status,
                                                                  uint32_t* __restrict__ tileCounter,
-                                                                 uint32_t* __restrict__ error) {
+                                                                 uint32_t* __restrict__ error,
+                                                                 long long lookbackLimit) {
     extern __shared__ __align__(16) unsigned char smem[];
     constexpr size_t kStageBytes = kSortTile * (sizeof(Key) > 4 ? sizeof(Key) : 4);
     Key* sKeys = reinterpret_cast<Key*>(smem);
@@ -354,7 +361,7 @@ __global__ void __launch_bounds__(kSortThreads, 3) radixOnesweep(Loader ld, Stor
                 const long long now = clock64();
                 if (waitStart < 0 || now < waitStart) {
                     waitStart = now;
-                } else if (now - waitStart > kLookbackLimitCycles) {
+                } else if (now - waitStart > lookbackLimit) {
                     failed = true;
                     break;
                 }
@@ -511,18 +518,22 @@ struct RadixScratch {
 };
 
 // One pass over `tiles` tiles (ceilDiv(count, kSortTile) for one segment; the segment table's total
-// otherwise). count bounds the elements of the pass (all segments together).
+// otherwise). count bounds the elements of the pass (all segments together). skipTiles > 0 is for the
+// test of the look-back's time-out only: tile numbers start there, so the first block's
+// predecessors never publish (their elements are still read: count covers them).
 template <class Key, class Loader, class Storer, class Segments = OneSegment>
 cudaError_t radixOnesweepPass(const Loader& ld, const Storer& st, const Segments& segs, uint32_t count,
                               uint32_t tiles, const uint32_t* digitBase, const RadixScratch& scratch,
-                              cudaStream_t stream) {
+                              cudaStream_t stream, long long lookbackLimit = kLookbackLimitCycles,
+                              uint32_t skipTiles = 0) {
     if (count == 0 || tiles == 0) return cudaSuccess;
     // A look-back word holds counts below 2^30: one segment at most that long (callers of the
     // segmented passes keep every segment below it).
     if (std::is_same<Segments, OneSegment>::value && count > kMaxSortCount) return cudaErrorInvalidValue;
-    // status words and the tile counter start at zero; the error word is kept.
-    SADCS_TRY(cudaMemsetAsync(scratch.status, 0, static_cast<size_t>(tiles) * 256 * 4, stream));
+    // status words and the tile counter start at zero (at skipTiles); the error word is kept.
+    SADCS_TRY(cudaMemsetAsync(scratch.status, 0, static_cast<size_t>(tiles + skipTiles) * 256 * 4, stream));
     SADCS_TRY(cudaMemsetAsync(scratch.control, 0, 4, stream));
+    if (skipTiles) SADCS_TRY(cudaMemsetAsync(scratch.control, static_cast<int>(skipTiles), 1, stream));
     constexpr size_t shared = radixSharedBytes(sizeof(Key));
     // The opt-in above 48 KiB of dynamic shared memory is per function and per device.
     static std::atomic<uint64_t> configured{0};
@@ -531,7 +542,7 @@ cudaError_t radixOnesweepPass(const Loader& ld, const Storer& st, const Segments
                                     cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(shared));
     }));
     return launch(radixOnesweep<Key, Loader, Storer, Segments>, tiles, kSortThreads, shared, stream, ld, st, segs,
-                  digitBase, scratch.status, scratch.control, scratch.control + 1);
+                  digitBase, scratch.status, scratch.control, scratch.control + 1, lookbackLimit);
 }
 
 // Stable LSD sort of (keys, vals) over bits [beginBit, endBit), ping-ponging with the alternates.

@@ -40,6 +40,7 @@ struct RankBuffers {
     uint32_t* scanScratch;  // scan scratch words (scanScratchWords(m))
     uint32_t* segScratch;   // segmented-sort scratch (segScratchWords(m))
     uint32_t* counter;      // device words: [0] list count, [4..7] segmented sort
+    uint32_t keyEntries;    // 64-bit entries of each key buffer (the pair arrays of a bucketed rank write)
 };
 
 
@@ -271,7 +272,8 @@ __global__ void __launch_bounds__(kRefineThreads) rankRefineApply(const uint32_t
                                                                   const uint32_t* __restrict__ agg,
                                                                   uint32_t* __restrict__ ranks,
                                                                   uint32_t* __restrict__ out,
-                                                                  uint32_t* __restrict__ grpOut, uint32_t writeAll) {
+                                                                  uint32_t* __restrict__ grpOut, uint32_t writeAll,
+                                                                  uint64_t* __restrict__ pairs) {
     __shared__ uint32_t warpTotals[32];
     __shared__ uint32_t incOld[kRefineThreads], incNew[kRefineThreads];
     const uint32_t base = blockIdx.x * kRefineTile + threadIdx.x * kRefineItems;
@@ -314,11 +316,97 @@ __global__ void __launch_bounds__(kRefineThreads) rankRefineApply(const uint32_t
         const uint32_t item = items[k];
         const uint32_t id = g[k] + (runNew - runOld);
         const bool kept = (keep >> k) & 1;
-        if (item < slots && (!kept || writeAll)) ranks[item] = id;
+        if (!kept || writeAll) {
+            if (pairs) {
+                // the pass's rank writes in list order: every element's, or the singletons' (an
+                // element's place among them is its index less the kept elements before it)
+                pairs[writeAll ? e : e - at] = item < slots ? (static_cast<uint64_t>(item) << 32) | id : ~uint64_t(0);
+            } else if (item < slots) {
+                ranks[item] = id;
+            }
+        }
         if (kept) {
             grpOut[at] = id;
             out[at++] = item;
         }
+    }
+}
+
+// ---- the rank writes of a large pass, in two steps --------------------------------------------
+//
+// The rank array is indexed by sample, so a pass's writes land at random places of it (each a
+// DRAM read and write of a sector once the array exceeds L2). A large pass instead writes its
+// (sample, rank) pairs in list order (rankRefineApply), rankPartitionPairs moves them into the
+// slice of the rank array they belong to (slice k: samples [k << shift, (k + 1) << shift); a pass
+// writes each sample at most once, so slice k of the pair array has room for all of its pairs),
+// and rankScatterPairs writes the slices one after another, each within an L2-sized part of the
+// rank array.
+constexpr uint32_t kRankSliceShift = 23;  // 8M samples = 32 MB of the rank array per slice
+constexpr uint32_t kMaxRankSlices = 128;
+constexpr int kPairThreads = 256;
+constexpr int kPairItems = 8;
+constexpr uint32_t kPairTile = kPairThreads * kPairItems;  // divides 2^kRankSliceShift
+// Passes writing fewer ranks than this write them directly.
+constexpr uint32_t kBucketedRankWrites = 8u << 20;
+
+inline uint32_t rankSliceShift(uint64_t slots) {
+    uint32_t shift = kRankSliceShift;
+    while ((slots >> shift) >= kMaxRankSlices) shift++;
+    return shift;
+}
+
+// pairs[0, count) -> dst, slice-major; count = u (every element wrote) or u less the kept total.
+// fill[k] (zeroed by the caller) counts the pairs placed in slice k.
+__global__ void __launch_bounds__(kPairThreads) rankPartitionPairs(const uint64_t* __restrict__ pairs, uint32_t u,
+                                                                   const uint32_t* __restrict__ keptTotal,
+                                                                   uint32_t writeAll, uint32_t shift,
+                                                                   uint32_t capacity, uint32_t* __restrict__ fill,
+                                                                   uint64_t* __restrict__ dst) {
+    __shared__ uint32_t count[kMaxRankSlices];
+    __shared__ uint32_t base[kMaxRankSlices];
+    for (uint32_t i = threadIdx.x; i < kMaxRankSlices; i += kPairThreads) count[i] = 0;
+    __syncthreads();
+    const uint32_t total = writeAll ? u : u - min(*keptTotal, u);
+    uint64_t v[kPairItems];
+    uint32_t local[kPairItems];
+    const uint64_t first = static_cast<uint64_t>(blockIdx.x) * kPairTile + threadIdx.x;
+#pragma unroll
+    for (int j = 0; j < kPairItems; j++) {
+        const uint64_t i = first + static_cast<uint64_t>(j) * kPairThreads;
+        v[j] = i < total ? __ldcs(pairs + i) : ~uint64_t(0);
+        const uint32_t t = static_cast<uint32_t>(v[j] >> 32);
+        if ((t >> shift) < kMaxRankSlices) {
+            local[j] = atomicAdd(&count[t >> shift], 1u);
+        } else {
+            v[j] = ~uint64_t(0);  // no pair, or a guarded out-of-range sample
+        }
+    }
+    __syncthreads();
+    for (uint32_t k = threadIdx.x; k < kMaxRankSlices; k += kPairThreads) {
+        if (count[k]) base[k] = atomicAdd(fill + k, count[k]);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < kPairItems; j++) {
+        if (v[j] == ~uint64_t(0)) continue;
+        const uint32_t k = static_cast<uint32_t>(v[j] >> 32) >> shift;
+        const uint64_t at = (static_cast<uint64_t>(k) << shift) + base[k] + local[j];
+        if (at < capacity && base[k] + local[j] < (1u << shift)) dst[at] = v[j];  // always, by construction
+    }
+}
+
+// Block b writes the pairs of dst[b * kPairTile, (b + 1) * kPairTile) that its slice holds.
+__global__ void __launch_bounds__(kPairThreads) rankScatterPairs(const uint64_t* __restrict__ dst, uint32_t shift,
+                                                                 uint32_t capacity, uint32_t slots,
+                                                                 const uint32_t* __restrict__ fill,
+                                                                 uint32_t* __restrict__ ranks) {
+    const uint64_t start = static_cast<uint64_t>(blockIdx.x) * kPairTile;
+    const uint32_t k = static_cast<uint32_t>(start >> shift);
+    const uint64_t end = min((static_cast<uint64_t>(k) << shift) + __ldg(fill + k), static_cast<uint64_t>(capacity));
+    for (uint64_t i = start + threadIdx.x; i < min(end, start + kPairTile); i += kPairThreads) {
+        const uint64_t v = __ldcs(dst + i);
+        const uint32_t t = static_cast<uint32_t>(v >> 32);
+        if (t < slots) ranks[t] = static_cast<uint32_t>(v);
     }
 }
 
@@ -333,6 +421,35 @@ inline int bitWidth(uint64_t x) {
         x >>= 1;
     }
     return b;
+}
+
+// Characters of the first character pass of one text, a global sort of every sample: the fewest
+// whole 8-bit radix passes whose key, tag included, holds enough characters for 2^(chars * bits)
+// to exceed 64 times the samples (on a text without repeats, about 1 sample in 64 then shares its
+// key with another; a repetitive text leaves its repeats to the later, segmented passes whatever
+// the width), and as many characters as those passes hold, at most keyChars. A narrower key is
+// taken only if it keeps at least kMinFirstPassChars characters: on the 3 GiB genome-like text
+// (2-bit codes) 21 characters in 6 passes took the ranking from 129.6 to 118.1 ms, while on the
+// 256 MiB natural-language-like text (6-bit codes) 6 characters in 5 passes left more suffixes in
+// word-sized repeats for the later passes (17.5 to 19.2 ms).
+constexpr uint32_t kMinFirstPassChars = 16;
+inline uint32_t firstPassChars(const TextSet& texts, uint64_t samples) {
+    auto width = [](uint32_t x) {
+        uint32_t w = 0;
+        while (x) {
+            w++;
+            x >>= 1;
+        }
+        return w;
+    };
+    const uint32_t b = texts.bits;
+    const uint32_t wantBits = static_cast<uint32_t>(bitWidth(samples)) + 6;
+    for (uint32_t passes = 1; passes <= 8; passes++) {
+        uint32_t c = std::min<uint32_t>(texts.keyChars, (8 * passes) / b);
+        while (c > 0 && c * b + width(c) > 8 * passes) c--;
+        if (c == texts.keyChars || c * b >= wantBits) return c >= kMinFirstPassChars ? c : texts.keyChars;
+    }
+    return texts.keyChars;
 }
 
 struct RankStats {
@@ -361,7 +478,12 @@ inline cudaError_t rankSample(const uint8_t* text, const TextSet& texts, uint32_
     uint64_t depth = 0;
     bool first = texts.count <= 1;  // one text: everything starts in one group, no group sort
     const int rankBits = bitWidth(static_cast<uint64_t>(live) + 1);
-    const int charBits = static_cast<int>(texts.keyChars * texts.bits + texts.tagBits);
+    // The first pass of one text may key fewer characters (fewer radix passes over every sample).
+    TextSet firstTexts = texts;
+    if (first) {
+        firstTexts.keyChars = firstPassChars(texts, live);
+        firstTexts.tagBits = static_cast<uint32_t>(bitWidth(firstTexts.keyChars));
+    }
     while (u > 0) {
         const bool doubling = depth >= kV;
         const uint32_t offset = doubling ? static_cast<uint32_t>((depth / kV) * kV) : static_cast<uint32_t>(depth);
@@ -371,9 +493,11 @@ inline cudaError_t rankSample(const uint8_t* text, const TextSet& texts, uint32_
         uint32_t* lstAlt = alt;
         uint64_t* key = b.key[0];
         uint64_t* keyAlt = b.key[1];
-        SADCS_TRY(launch(rankMakeKeys, blocks256(u), 256, 0, stream, text, ranks, texts, lst, key, u, offset,
+        const TextSet& passTexts = first ? firstTexts : texts;
+        SADCS_TRY(launch(rankMakeKeys, blocks256(u), 256, 0, stream, text, ranks, passTexts, lst, key, u, offset,
                          doubling ? 1 : 0));
-        const int keyBits = doubling ? rankBits : charBits;
+        const int keyBits = doubling ? rankBits
+                                     : static_cast<int>(passTexts.keyChars * passTexts.bits + passTexts.tagBits);
         if (first) {
             // Everything in one group: one global sort by subkey.
             SADCS_TRY(radixSortPairs<uint64_t>(key, keyAlt, lst, lstAlt, u, 0, keyBits, b.scratch, stream));
@@ -390,12 +514,24 @@ inline cudaError_t rankSample(const uint8_t* text, const TextSet& texts, uint32_
             SADCS_TRY(segmentedSort(b.grp, u, key, lst, keyAlt, lstAlt, keyBits, sb, hostCounter + 8, stream));
         }
         // The next pass reads ranks of other samples when it is a doubling round.
-        const bool writeAll = doubling || depth + texts.keyChars >= kV;
+        const bool writeAll = doubling || depth + passTexts.keyChars >= kV;
         const uint32_t refineTiles = ceilDiv(u, kRefineTile);
         SADCS_TRY(launch(rankRefineReduce, refineTiles, kRefineThreads, 0, stream, b.grp, key, u, refineTiles, b.aux1));
         SADCS_TRY(launch(rankRefineScan, 1, 256, 0, stream, b.aux1, refineTiles, b.counter));
+        // A large pass writes its ranks through pairs in the free key buffer (bucketed, below).
+        const bool bucketed = u >= kBucketedRankWrites && slots <= b.keyEntries;
         SADCS_TRY(launch(rankRefineApply, refineTiles, kRefineThreads, 0, stream, b.grp, key, lst, u, slots, refineTiles,
-                         b.aux1, ranks, lstAlt, b.aux2, writeAll ? 1u : 0u));
+                         b.aux1, ranks, lstAlt, b.aux2, writeAll ? 1u : 0u, bucketed ? keyAlt : nullptr));
+        if (bucketed) {
+            // the sorted keys are dead now: they become the slice-major pair array
+            const uint32_t shift = rankSliceShift(slots);
+            uint32_t* fill = b.scratch;  // the first sort's digit bases, dead after it
+            SADCS_TRY(cudaMemsetAsync(fill, 0, kMaxRankSlices * sizeof(uint32_t), stream));
+            SADCS_TRY(launch(rankPartitionPairs, ceilDiv(u, kPairTile), kPairThreads, 0, stream, keyAlt, u, b.counter,
+                             writeAll ? 1u : 0u, shift, b.keyEntries, fill, key));
+            SADCS_TRY(launch(rankScatterPairs, ceilDiv(slots, kPairTile), kPairThreads, 0, stream, key, shift,
+                             b.keyEntries, slots, fill, ranks));
+        }
         std::swap(b.grp, b.aux2);  // the kept elements' ids are the next pass's groups
         SADCS_TRY(cudaMemcpyAsync(hostCounter, b.counter, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
         SADCS_TRY(cudaMemcpyAsync(hostCounter + 1, error, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
@@ -413,7 +549,7 @@ inline cudaError_t rankSample(const uint8_t* text, const TextSet& texts, uint32_
             depth += offset;
         } else {
             stats.characterPasses++;
-            depth += texts.keyChars;
+            depth += passTexts.keyChars;
         }
         first = false;
     }

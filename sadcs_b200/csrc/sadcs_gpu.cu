@@ -620,6 +620,7 @@ int construct(sadcs_gpu_context* c, const Batch& b, Io& io, cudaStream_t stream,
     rb.scanScratch = reinterpret_cast<uint32_t*>(slab + L.scanScratch);
     rb.segScratch = reinterpret_cast<uint32_t*>(slab + L.segScratch);
     rb.counter = reinterpret_cast<uint32_t*>(slab + L.counter);
+    rb.keyEntries = static_cast<uint32_t>(std::min(L.key1 - L.key0, L.grp - L.key1) / 8);
     RankStats rankStats;
     if ((error = rankSample(text, texts, static_cast<uint32_t>(b.slots), static_cast<uint32_t>(b.live), dSampleBase,
                             static_cast<uint32_t>(b.longest), ranks, rb, c->hostWords, stream, rankStats)) !=
@@ -1323,6 +1324,57 @@ int sadcs_gpu_check_bwt_host(const uint8_t* text, int64_t n, const uint8_t* bwt,
                                primary, bad_index, in.stream);
 }
 
+int sadcs_gpu_test_lookback_timeout(int64_t limit_cycles, uint32_t* error_word) {
+    tLastError[0] = '\0';
+    if (error_word) *error_word = 0;
+    if (limit_cycles <= 0 || limit_cycles > kLookbackLimitCycles) {
+        setError("limit of %lld cycles out of range (1 to %lld)", static_cast<long long>(limit_cycles),
+                 static_cast<long long>(kLookbackLimitCycles));
+        return SADCS_FAILED;
+    }
+    // One radix pass of two tiles' elements in which a single block takes tile 1: tile 0 is never
+    // taken, so its status words stay zero and the block's look-back waits on them until the limit.
+    constexpr uint32_t count = 2 * kSortTile;
+    cudaStream_t st = nullptr;
+    cudaError_t error = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    if (error != cudaSuccess) return failed("cudaStreamCreate", error);
+    uint64_t* keys = nullptr;
+    uint32_t* vals = nullptr;
+    uint32_t* scratch = nullptr;
+    const size_t keyBytes = 2 * 8 * static_cast<size_t>(count), valBytes = 2 * 4 * static_cast<size_t>(count);
+    const size_t scratchBytes = 4 * radixScratchWords(count);
+    uint32_t word = 0;
+    if ((error = cudaMallocAsync(&keys, keyBytes, st)) == cudaSuccess &&
+        (error = cudaMallocAsync(&vals, valBytes, st)) == cudaSuccess &&
+        (error = cudaMallocAsync(&scratch, scratchBytes, st)) == cudaSuccess &&
+        (error = cudaMemsetAsync(keys, 0, keyBytes, st)) == cudaSuccess &&
+        (error = cudaMemsetAsync(vals, 0, valBytes, st)) == cudaSuccess &&
+        (error = cudaMemsetAsync(scratch, 0, scratchBytes, st)) == cudaSuccess) {
+        const RadixScratch radix(scratch, count);
+        SortLoader<uint64_t> ld{keys, vals, 0};
+        SortStorer<uint64_t> out{keys + count, vals + count, count};
+        error = radixOnesweepPass<uint64_t>(ld, out, OneSegment{count}, count, 1, radix.digitBase, radix, st,
+                                            static_cast<long long>(limit_cycles), 1);
+        if (error == cudaSuccess) {
+            error = cudaMemcpyAsync(&word, radix.control + 1, sizeof word, cudaMemcpyDeviceToHost, st);
+        }
+        if (error == cudaSuccess) error = cudaStreamSynchronize(st);
+    }
+    if (keys) cudaFreeAsync(keys, st);
+    if (vals) cudaFreeAsync(vals, st);
+    if (scratch) cudaFreeAsync(scratch, st);
+    cudaStreamSynchronize(st);
+    cudaStreamDestroy(st);
+    if (error != cudaSuccess) return failed("look-back time-out test", error);
+    if (error_word) *error_word = word;
+    if (word) {
+        setError("radix look-back gave up after %lld cycles (error word %u): nothing was stored",
+                 static_cast<long long>(limit_cycles), word);
+        return SADCS_FAILED;
+    }
+    return SADCS_OK;
+}
+
 int sadcs_gpu_lcp(const uint8_t* d_text, int64_t n, const uint32_t* d_sa, uint32_t* d_lcp, void* stream) {
     tLastError[0] = '\0';
     if (n <= 0) return SADCS_OK;
@@ -1381,6 +1433,7 @@ int sadcs_gpu_rank_sample(const uint8_t* text, int64_t n, uint32_t* ranks, sadcs
         rb.scanScratch = reinterpret_cast<uint32_t*>(c->slab + L.scanScratch);
         rb.segScratch = reinterpret_cast<uint32_t*>(c->slab + L.segScratch);
         rb.counter = reinterpret_cast<uint32_t*>(c->slab + L.counter);
+        rb.keyEntries = static_cast<uint32_t>(std::min(L.key1 - L.key0, L.grp - L.key1) / 8);
         TextSet texts{};
         texts.count = 1;
         texts.oneEnd = static_cast<uint32_t>(length);
