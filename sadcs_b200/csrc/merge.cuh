@@ -25,17 +25,39 @@
 namespace sadcs {
 
 constexpr uint32_t kMergeG = 32;
-// Rows every R splitters; tiles of at most G * R + 6 * (G - 1) + 1 records (1467 at R = 40). R sets the
-// tile's shared memory and so the blocks per SM; the build may override it (tuning).
+
+// Tile shape, by the number W of 64-bit code words a record keeps (the code width): rows every R
+// splitters, so a tile holds at most G * R + 6 * (G - 1) + 1 records, and its threads. R sets the
+// tile's shared memory and so the tiles per SM. One-word records (2-bit codes: 17 bytes) leave
+// shared memory to spare and take larger tiles: on the 3 GiB genome-like text the final level took
+// 170.3 ms at R = 64 with 384 threads (5 tiles per SM), 174.5 at R = 80 with 512 threads (4),
+// 176.6 at R = 40 with 256 threads (8) and 188.6 at R = 40 with 384 (4); wider records (33 bytes for
+// 6-bit codes) fill it: the 256 MiB natural-language-like text took 14.0 ms at R = 40, 14.6 at 56
+// and 17.1 at 64 (tuning).
 #ifndef SADCS_MERGE_R
 #define SADCS_MERGE_R 40
 #endif
-constexpr uint32_t kMergeR = SADCS_MERGE_R;
-constexpr uint32_t kMergeCap = kMergeG * kMergeR + 6 * (kMergeG - 1) + 1;
 #ifndef SADCS_MERGE_THREADS
 #define SADCS_MERGE_THREADS 384
 #endif
-constexpr int kMergeThreads = SADCS_MERGE_THREADS;  // threads per tile (tuning)
+#ifndef SADCS_MERGE_R_W1
+#define SADCS_MERGE_R_W1 64
+#endif
+#ifndef SADCS_MERGE_THREADS_W1
+#define SADCS_MERGE_THREADS_W1 384
+#endif
+__host__ __device__ constexpr uint32_t mergeCap(uint32_t r) {
+    return kMergeG * r + 6 * (kMergeG - 1) + 1;
+}
+__host__ __device__ constexpr uint32_t mergeR(int words) {
+    return words == 1 ? SADCS_MERGE_R_W1 : SADCS_MERGE_R;
+}
+__host__ __device__ constexpr int mergeThreads(int words) {
+    return words == 1 ? SADCS_MERGE_THREADS_W1 : SADCS_MERGE_THREADS;
+}
+// The smallest R of any shape: the most rows a plan can have (memory plans bound with it).
+constexpr uint32_t kMergeRMin = SADCS_MERGE_R < SADCS_MERGE_R_W1 ? SADCS_MERGE_R : SADCS_MERGE_R_W1;
+static_assert(mergeCap(SADCS_MERGE_R) <= 65535 && mergeCap(SADCS_MERGE_R_W1) <= 65535, "u16 record indices");
 constexpr uint32_t kNoList = 0xFFFFFFFFu;
 constexpr int kMaxLevels = 10;
 
@@ -172,7 +194,7 @@ __device__ __forceinline__ int listOfElement(const uint32_t* seg, uint32_t e) {
 // the number of elements before the windows (t.base), the window indices of the tile's two
 // splitters (t.loIdx, t.hiIdx; kNoList for the ends of the level) and whether the window set fits
 // (t.bad otherwise, never by construction).
-__device__ __forceinline__ void planTileWindows(const MergeArgs& a, MergeTileInfo& t) {
+__device__ __forceinline__ void planTileWindows(const MergeArgs& a, uint32_t cap, MergeTileInfo& t) {
     const uint32_t* st = a.level.start;
     const uint32_t b = threadIdx.x & 31;
     uint32_t w = 0, e = 0;
@@ -226,7 +248,7 @@ __device__ __forceinline__ void planTileWindows(const MergeArgs& a, MergeTileInf
         t.size = size;
         t.loIdx = loList == kNoList ? kNoList : loStart;
         t.hiIdx = hiList == kNoList ? kNoList : hiEnd - 1;
-        t.bad = size > kMergeCap;
+        t.bad = size > cap;
     }
 }
 
@@ -306,11 +328,12 @@ struct MergePlan {
     size_t rows = 0;
 };
 
-inline MergePlan planMerge(const uint32_t* classStart) {
+// r: the tile shape's row spacing (mergeR of the texts' code width).
+inline MergePlan planMerge(const uint32_t* classStart, uint32_t r) {
     MergePlan p;
     for (int b = 0; b <= kClasses; b++) p.start[0][b] = classStart[b];
     int L = 0;
-    while (p.start[L][kClasses] > kMergeCap && L + 1 < kMaxLevels) {
+    while (p.start[L][kClasses] > mergeCap(r) && L + 1 < kMaxLevels) {
         p.listWord[L + 1] = p.splitterWords;
         for (int b = 0; b < kClasses; b++) {
             const uint32_t len = p.start[L][b + 1] - p.start[L][b];
@@ -321,7 +344,7 @@ inline MergePlan planMerge(const uint32_t* classStart) {
     }
     p.top = L;
     for (int l = 0; l < L; l++) {
-        p.tiles[l] = (p.start[l + 1][kClasses] + kMergeR - 1) / kMergeR;
+        p.tiles[l] = (p.start[l + 1][kClasses] + r - 1) / r;
         p.rowIndex[l] = p.rows;
         p.rows += p.tiles[l] + 1;
     }

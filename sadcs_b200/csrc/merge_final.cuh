@@ -42,6 +42,7 @@ __host__ __device__ constexpr int finalWords(uint32_t bits) {
 
 template <int W, bool kMulti>
 struct FinalTile {
+    static constexpr uint32_t kMergeCap = mergeCap(mergeR(W));
     static constexpr size_t kPerRecord = 8 * W + 4 + (kMulti ? 4 : 0) + 2 + 2 + 1;
     static constexpr size_t sharedBytes() { return kMergeCap * kPerRecord + 64; }
     uint64_t* words;
@@ -106,8 +107,8 @@ __device__ __forceinline__ bool headLess(const FinalTile<W, kMulti>& s, const Fi
 #pragma unroll
         for (int w = 1; w < W; w++) {
             if (lim <= 64u * w) break;
-            x = s.words[w * kMergeCap + a.idx];
-            y = s.words[w * kMergeCap + b.idx];
+            x = s.words[w * s.kMergeCap + a.idx];
+            y = s.words[w * s.kMergeCap + b.idx];
             if (lim < 64u * (w + 1)) {
                 const uint64_t mk = ~uint64_t(0) << (64u * (w + 1) - lim);
                 x &= mk;
@@ -119,7 +120,7 @@ __device__ __forceinline__ bool headLess(const FinalTile<W, kMulti>& s, const Fi
         if (a.w0 != b.w0) return a.w0 < b.w0;
 #pragma unroll
         for (int w = 1; w < W; w++) {
-            const uint64_t x = s.words[w * kMergeCap + a.idx], y = s.words[w * kMergeCap + b.idx];
+            const uint64_t x = s.words[w * s.kMergeCap + a.idx], y = s.words[w * s.kMergeCap + b.idx];
             if (x != y) return x < y;
         }
     }
@@ -148,7 +149,8 @@ template <int W, bool kMulti, bool kIdentity>
 __device__ __forceinline__ void finalLevel(const FinalTile<W, kMulti>& s, const uint16_t* src, uint16_t* dst,
                                            const uint32_t* mb, int merges, uint32_t size, uint32_t n,
                                            uint32_t bits) {
-    const uint32_t chunk = max((size + kMergeThreads - 1) / kMergeThreads, static_cast<uint32_t>(SADCS_MERGE_MIN_CHUNK));
+    constexpr uint32_t kThreads = mergeThreads(W);
+    const uint32_t chunk = max((size + kThreads - 1) / kThreads, static_cast<uint32_t>(SADCS_MERGE_MIN_CHUNK));
     uint32_t at = threadIdx.x * chunk;
     const uint32_t stopAll = min(at + chunk, size);
     int m = 0;
@@ -191,12 +193,11 @@ __device__ __forceinline__ void finalLevel(const FinalTile<W, kMulti>& s, const 
     }
 }
 
-// Tiles resident per SM the register budget is set for. One code word per record leaves room in
-// shared memory for 5 tiles of 384 threads, but at the 32 registers that allows the kernel spills:
-// 4 tiles without spills were 3% faster on the 3 GiB genome-like text (168.3 against 173.2 ms);
-// wider records fill shared memory at 4 (tuning).
+// Tiles resident per SM the register budget is set for: as many as the SM's 2048 threads hold for
+// one-word records (their shared memory allows more), 4 for wider records, which fill shared
+// memory at 4 (tuning).
 #ifndef SADCS_MERGE_TILES_W1
-#define SADCS_MERGE_TILES_W1 4
+#define SADCS_MERGE_TILES_W1 (2048 / SADCS_MERGE_THREADS_W1)
 #endif
 template <int W>
 constexpr int mergeTilesPerSm() {
@@ -206,7 +207,10 @@ constexpr int mergeTilesPerSm() {
 // kFinal: the last level, writing the SA and the BWT; otherwise an upper level, writing the rows
 // (every R-th element of the merged order with its per-list counts) that bound the tiles below.
 template <int W, bool kMulti, bool kFinal>
-__global__ void __launch_bounds__(kMergeThreads, mergeTilesPerSm<W>()) mergeTree(MergeArgs a) {
+__global__ void __launch_bounds__(mergeThreads(W), mergeTilesPerSm<W>()) mergeTree(MergeArgs a) {
+    constexpr int kMergeThreads = mergeThreads(W);
+    constexpr uint32_t kMergeR = mergeR(W);
+    constexpr uint32_t kMergeCap = FinalTile<W, kMulti>::kMergeCap;
     extern __shared__ __align__(16) unsigned char smem[];
     FinalTile<W, kMulti> s;
     s.carve(smem, a.ranks);
@@ -214,7 +218,7 @@ __global__ void __launch_bounds__(kMergeThreads, mergeTilesPerSm<W>()) mergeTree
     __shared__ uint32_t sLo, sHi;
     __shared__ uint32_t bounds[3 * 7];  // the tree's merges: 4 + 2 + 1 triples of window offsets
     if (threadIdx.x < 32) {
-        planTileWindows(a, t);
+        planTileWindows(a, kMergeCap, t);
         __syncwarp();
         // (0,1) (2,3) (4,5) (6,-), then (01,23) (45,6), then (0123,456): indices into t.seg, 3 bits
         // each (a register constant: a table indexed by the lane would live in local memory)
@@ -409,7 +413,7 @@ inline cudaError_t launchTreeFor(const MergeArgs& args, uint32_t tiles, cudaStre
 #endif
         return cudaSuccess;
     }));
-    return launch(mergeTree<W, kMulti, kFinal>, tiles, kMergeThreads, shared, stream, args);
+    return launch(mergeTree<W, kMulti, kFinal>, tiles, mergeThreads(W), shared, stream, args);
 }
 
 template <bool kMulti, bool kFinal>

@@ -226,13 +226,22 @@ struct ManySegments {
 // element takes part, its key and digit (load), and later its value (value, called again for the
 // same elements only, so that values are not held in registers through ranking and look-back).
 // Storers write keys (when kKeys) and values at output positions.
-// Tiles resident per SM the register budget is set for (tuning).
+// Tiles resident per SM the register budget is set for: a loader may ask for its own number
+// (kTilesPerSm), otherwise SADCS_SORT_TILES (tuning).
 #ifndef SADCS_SORT_TILES
 #define SADCS_SORT_TILES 3
 #endif
+template <class Loader, class = void>
+struct SortTilesPerSm {
+    static constexpr int value = SADCS_SORT_TILES;
+};
+template <class Loader>
+struct SortTilesPerSm<Loader, std::void_t<decltype(Loader::kTilesPerSm)>> {
+    static constexpr int value = Loader::kTilesPerSm;
+};
 
 template <class Key, class Loader, class Storer, class Segments = OneSegment>
-__global__ void __launch_bounds__(kSortThreads, SADCS_SORT_TILES) radixOnesweep(Loader ld, Storer st, Segments segs,
+__global__ void __launch_bounds__(kSortThreads, SortTilesPerSm<Loader>::value) radixOnesweep(Loader ld, Storer st, Segments segs,
                                                                  const uint32_t* __restrict__ digitBase,
                                                                  uint32_t* __restrict__ status,
                                                                  uint32_t* __restrict__ tileCounter,

@@ -121,7 +121,7 @@ bool planBatch(const uint64_t* lengths, uint32_t count, Batch& b) {
     b.outputs = outputs;
     b.classTables.assign(ClassTables::words(count), 0);
     planClasses(lengths, count, b.classTables.data(), b.classes);
-    b.merge = planMerge(b.classes.start);
+    b.merge = planMerge(b.classes.start, kMergeRMin);  // the most rows any tile shape needs (memory plan)
     return true;
 }
 
@@ -166,10 +166,10 @@ Extent extentBound(uint64_t total, uint32_t texts) {
     e.outputs = total;
     e.largestClass = e.live;
     uint64_t words = 0, rows = 0, level = total;
-    while (level > kMergeCap) {
+    while (level > mergeCap(kMergeRMin)) {
         const uint64_t next = level / kMergeG + kClasses;
         words += next + 64;
-        rows += (next + kMergeR - 1) / kMergeR + 1;
+        rows += (next + kMergeRMin - 1) / kMergeRMin + 1;
         level = next;
     }
     e.splitterWords = words;
@@ -662,7 +662,9 @@ int construct(sadcs_gpu_context* c, const Batch& b, Io& io, cudaStream_t stream,
     uint32_t* sa = saPieces ? nullptr
                             : (io.outSa ? io.outSa : (io.wantSa ? reinterpret_cast<uint32_t*>(slab + L.sa) : nullptr));
     uint8_t* bwt = bwtPieces ? nullptr : (io.outBwt ? io.outBwt : (io.wantBwt ? slab + L.bwt : nullptr));
-    if ((error = mergeClasses(text, ranks, texts, lists, b.merge, classTables.rowBase, dOutBase, dRowZero,
+    // The merge's tile shape follows the code width, known now (the memory plan bounds every shape).
+    const MergePlan mergePlan = planMerge(b.classes.start, mergeR(finalWords(texts.bits)));
+    if ((error = mergeClasses(text, ranks, texts, lists, mergePlan, classTables.rowBase, dOutBase, dRowZero,
                               reinterpret_cast<uint32_t*>(slab + L.splitters),
                               reinterpret_cast<MergeRow*>(slab + L.rows), sa, bwt,
                               reinterpret_cast<uint32_t*>(slab + L.mergeCounter), c->hostWords, stream,

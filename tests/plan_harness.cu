@@ -24,7 +24,7 @@ int checkPlacement(const Batch& b, const uint64_t* lengths, uint32_t count, int6
     if (classTotal != outputs || b.classes.start[1] != live) return 8;  // classes partition the positions
     detail[0] = b.merge.top;
     detail[1] = b.merge.start[b.merge.top][kClasses];
-    if (detail[1] > static_cast<int64_t>(kMergeCap)) return 9;  // the top merge level fits one tile
+    if (detail[1] > static_cast<int64_t>(mergeCap(kMergeRMin))) return 9;  // the top merge level fits one tile
     return 0;
 }
 

@@ -133,7 +133,7 @@ def comb_assign(rng, sizes):
     return np.concatenate(runs)
 
 
-@pytest.mark.parametrize("R", [26, 40])
+@pytest.mark.parametrize("R", [26, 40, 80])  # 40: records of several code words; 80: of one
 @pytest.mark.parametrize("assign", [random_assign, block_assign, staircase_assign, comb_assign])
 def test_tiles_fit_and_cover_the_output(R, assign):
     rng = np.random.default_rng(11)
@@ -147,4 +147,5 @@ def test_tiles_with_empty_and_tiny_lists():
         owner = np.repeat(np.arange(CLASSES), sizes)
         rng.shuffle(owner)
         lists = [np.flatnonzero(owner == b).astype(np.int64) for b in range(CLASSES)]
-        check_tiling(lists, 40)
+        for R in (40, 80):
+            check_tiling(lists, R)
