@@ -518,6 +518,13 @@ def run_ours(args, world, rank, local) -> None:
         line["cpu_baseline"] = cpu_baseline(text[:args.cpu_sample_mib << 20])
     if world == 1 and args.reference_gpu_steps > 0:
         line["reference_gpu"] = reference_gpu_record(args, d_text, ctx, text, stream)
+    if world == 1 and args.batch_steps > 0:
+        # the batched configuration beside the headline (its own workload: 4096 uneven texts)
+        ctx.close()
+        del d_text, d_sa, d_bwt
+        torch.cuda.empty_cache()
+        line["batch"] = {"workload": "batch4096", "description": BATCH_DESC,
+                         **measure_batch(args, 1, 0, local, args.batch_steps, 2, clocks=False)}
     print(json.dumps(line), flush=True)
 
 
@@ -687,80 +694,103 @@ def run_lcp(args, world, rank, local) -> None:
     print(json.dumps(line), flush=True)
 
 
-def run_batch(args, world, rank, local) -> None:
-    """Config 4: many uneven texts in one construction, against one construction per text."""
+def measure_batch(args, world, rank, local, steps: int, warmup: int, clocks: bool = True) -> dict:
+    """Config 4: many uneven texts in one construction (sadcs_gpu_build_batch_device), against one
+    construction per text on a bounded sample of the same texts (device-resident both). Every
+    sampled text's SA, BWT and primary from the batch are checked against its own construction."""
     import torch
 
     import sadcs_b200 as sa
     from sadcs_b200 import workloads as W
 
     torch.cuda.set_device(local)
+    device = f"cuda:{local}"
     texts = W.batch_texts(args.batch_count * world, lo=1 << 10, hi=4 << 20, seed=4,
                           indices=batch_share(args.batch_count, world, rank))
     lengths = [len(t) for t in texts]
-    total = sum(lengths)
-    packed = torch.from_numpy(np.concatenate(texts)).to(f"cuda:{local}")
-    d_sa = torch.empty(total, dtype=torch.int32, device=f"cuda:{local}")
-    d_bwt = torch.empty(total, dtype=torch.uint8, device=f"cuda:{local}")
+    offsets = np.concatenate([[0], np.cumsum(lengths)]).astype(np.int64)
+    total = int(offsets[-1])
+    packed = torch.from_numpy(np.concatenate(texts)).to(device)
+    d_sa = torch.empty(total, dtype=torch.int32, device=device)
+    d_bwt = torch.empty(total, dtype=torch.uint8, device=device)
     ctx = sa.Context(total, max_texts=len(texts))
     stream = torch.cuda.current_stream()
     stats = sa.Stats()
+    primaries = []
 
     def step():
-        return sa.build_batch_device(packed.data_ptr(), lengths, d_sa.data_ptr(), d_bwt.data_ptr(), context=ctx,
-                                     stream=stream.cuda_stream, stats=stats)
+        primaries[:] = sa.build_batch_device(packed.data_ptr(), lengths, d_sa.data_ptr(), d_bwt.data_ptr(),
+                                             context=ctx, stream=stream.cuda_stream, stats=stats)
 
-    for _ in range(max(args.warmup, 0)):
+    for _ in range(max(warmup, 0)):
         step()
     torch.cuda.synchronize()
     sampler = ClockSampler(None)
-    sampler.start()
+    if clocks:
+        sampler.start()
     barrier(world)
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     launches = 0
     start.record(stream)
-    for _ in range(args.steps):
+    for _ in range(steps):
         step()
         launches += int(stats.kernel_launches)
     stop.record(stream)
     torch.cuda.synchronize()
     barrier(world)
-    clocks = sampler.stop()
-    ms = start.elapsed_time(stop) / args.steps
+    clock_record = sampler.stop() if clocks else None
+    ms = start.elapsed_time(stop) / steps
     ms_max = max_over_ranks(ms, world)
     value = sum_over_ranks(float(total), world) / MIB / (ms_max / 1e3)
     texts_total = sum_over_ranks(float(len(texts)), world)
+    ctx.close()
 
     # The plain path: one construction per text (a bounded sample of the same texts), device-resident.
-    sample = texts[:: max(1, len(texts) // args.plain_sample)][: args.plain_sample]
-    one = sa.Context(max(len(t) for t in sample))
-    plain_bytes, plain_ms = 0, 0.0
-    for t in sample:
-        d_t = torch.from_numpy(t).to(f"cuda:{local}")
+    picks = list(range(0, len(texts), max(1, len(texts) // args.plain_sample)))[: args.plain_sample]
+    longest = max(lengths[i] for i in picks)
+    one = sa.Context(longest)
+    p_sa = torch.empty(longest, dtype=torch.int32, device=device)
+    p_bwt = torch.empty(longest, dtype=torch.uint8, device=device)
+    plain_bytes, plain_ms, same = 0, 0.0, True
+    for i in picks:
+        lo, hi = int(offsets[i]), int(offsets[i + 1])
         a = torch.cuda.Event(enable_timing=True)
         b = torch.cuda.Event(enable_timing=True)
         a.record(stream)
-        sa.build_device(d_t.data_ptr(), len(t), d_sa.data_ptr(), d_bwt.data_ptr(), context=one,
-                        stream=stream.cuda_stream)
+        p = sa.build_device(packed[lo:hi].data_ptr(), lengths[i], p_sa.data_ptr(), p_bwt.data_ptr(), context=one,
+                            stream=stream.cuda_stream)
         b.record(stream)
         torch.cuda.synchronize()
         plain_ms += a.elapsed_time(b)
-        plain_bytes += len(t)
+        plain_bytes += lengths[i]
+        same = same and p == primaries[i] and torch.equal(p_sa[:hi - lo], d_sa[lo:hi]) and \
+            torch.equal(p_bwt[:hi - lo], d_bwt[lo:hi])
     one.close()
     plain = plain_bytes / MIB / (plain_ms / 1e3)
+    return {"value": round(value, 3), "unit": UNIT, "ms_per_step": round(ms_max, 3), "steps": steps,
+            "warmup": warmup, "texts": len(texts), "total_bytes": total,
+            "texts_per_s": round(texts_total / (ms_max / 1e3), 1),
+            "plain_one_text_per_launch": {"value": round(plain, 3), "unit": UNIT, "texts": len(picks),
+                                          "texts_per_s": round(len(picks) / (plain_ms / 1e3), 1)},
+            "speedup_vs_plain": round(value / world / plain, 2), "gpu_launches": launches,
+            "sample_equal_to_plain": bool(same), "clocks": clock_record}
+
+
+def run_batch(args, world, rank, local) -> None:
+    """--workload batch4096: measure_batch as the line's own figures."""
+    r = measure_batch(args, world, rank, local, args.steps, args.warmup)
     if rank == 0:
         print(json.dumps({
-            "metric": "batched input MB/s (bit-exact SA+BWT per text)", "value": round(value, 3), "unit": UNIT,
-            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_max, 3),
+            "metric": "batched input MB/s (bit-exact SA+BWT per text)", "value": r["value"], "unit": UNIT,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms_per_step"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
-            "config": {"workload": "batch4096", "description": BATCH_DESC, "texts": len(texts), "total_bytes": total,
-                       "l2": "inputs larger than L2",
+            "config": {"workload": "batch4096", "description": BATCH_DESC, "texts": r["texts"],
+                       "total_bytes": r["total_bytes"], "l2": "inputs larger than L2",
                        "parallelism": ("one batch of %d texts per GPU, partitioned by footprint (longest first)"
                                        % args.batch_count) if world > 1 else "single GPU"},
-            "texts_per_s": round(texts_total / (ms_max / 1e3), 1),
-            "plain_one_text_per_launch": {"value": round(plain, 3), "unit": UNIT, "texts": len(sample),
-                                          "texts_per_s": round(len(sample) / (plain_ms / 1e3), 1)},
-            "speedup_vs_plain": round(value / world / plain, 2), "clocks": clocks, "gpu_launches": launches,
+            "texts_per_s": r["texts_per_s"], "plain_one_text_per_launch": r["plain_one_text_per_launch"],
+            "speedup_vs_plain": r["speedup_vs_plain"], "sample_equal_to_plain": r["sample_equal_to_plain"],
+            "clocks": r["clocks"], "gpu_launches": r["gpu_launches"],
         }), flush=True)
 
 
@@ -868,11 +898,20 @@ def run_serve(args, world, rank, local) -> None:
         constructions -= constructions0
         launches -= launches0
         total_bytes = float(lengths.sum())
+        lat = np.array(latencies)
+        small = lengths <= (64 << 20)
+
+        def pct(mask, q):
+            return round(float(np.percentile(lat[mask], q)) * 1e3, 2) if mask.any() else None
+
         results.append({"offered_req_s": load, "requests": count, "req_s": round(count / elapsed, 2),
                         "mib_s": round(total_bytes / MIB / elapsed, 2),
                         "offered_mib_s": round(total_bytes / MIB / float(arrivals[-1]), 2),
                         "p50_ms": round(float(np.percentile(latencies, 50)) * 1e3, 2),
                         "p99_ms": round(float(np.percentile(latencies, 99)) * 1e3, 2),
+                        "up_to_64mib": {"requests": int(small.sum()), "p50_ms": pct(small, 50), "p99_ms": pct(small, 99)},
+                        "at_1gib": {"requests": int((~small).sum()), "p50_ms": pct(~small, 50),
+                                    "max_ms": round(float(lat[~small].max()) * 1e3, 2) if (~small).any() else None},
                         "mean_batch": round(float(np.mean(batch_sizes)), 2), "constructions": constructions,
                         "gpu_launches": launches})
         if first is None:
@@ -944,6 +983,8 @@ def main() -> None:
     p.add_argument("--e2e-steps", type=int, default=3)
     p.add_argument("--reference-gpu-steps", type=int, default=2,
                    help="steps of the reference CUDA build in the line's reference_gpu record (0: none)")
+    p.add_argument("--batch-steps", type=int, default=3,
+                   help="steps of the batch4096 record in the default line's `batch` (0: none)")
     p.add_argument("--no-e2e", dest="e2e", action="store_false")
     p.add_argument("--no-verify", dest="verify", action="store_false")
     args = p.parse_args()

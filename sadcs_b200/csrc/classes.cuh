@@ -167,47 +167,58 @@ __global__ void classScatterPairs(const uint64_t* __restrict__ pairs, uint32_t l
     if (r < live) list[r] = static_cast<uint32_t>(v);
 }
 
-// Codes of the 8 characters before p: byte i holds the code of T[p - 1 - i] (0 before position 0),
-// from one 64-bit window of the code stream (b <= 8, so 8 codes fit in it).
-__device__ __forceinline__ uint64_t codesBefore(const TextSet& texts, uint32_t p) {
+// The class passes consume one character of an element's chain each: pass d keys class d - 1's
+// element p by the code of T[p - 1] and hands p - 1 the rest. Six passes follow class 0, so a
+// chain holds the codes of the kChainChars characters before p, b bits each: bits [i*b, (i+1)*b)
+// hold the code of T[p - 1 - i] (0 before position 0). The chain travels as the sort key in the
+// narrowest word that holds 6b bits: 16 bits for 2-bit codes (DNA), 32 for up to 5, 64 otherwise.
+constexpr int kChainChars = kClasses - 1;
+
+template <class Chain>
+__device__ __forceinline__ Chain codesBefore(const TextSet& texts, uint32_t p) {
     const uint32_t b = texts.bits;
-    const uint32_t first = p >= 8 ? p - 8 : 0;
-    const uint64_t window = streamBits(texts.packed, static_cast<uint64_t>(first) * b);
+    const uint32_t first = p >= kChainChars ? p - kChainChars : 0;
+    const uint64_t window = streamBits(texts.packed, static_cast<uint64_t>(first) * b);  // >= 8 codes
     const uint64_t mask = (uint64_t(1) << b) - 1;
     uint64_t chain = 0;
 #pragma unroll
-    for (int i = 0; i < 8; i++) {
+    for (int i = 0; i < kChainChars; i++) {
         const int at = static_cast<int>(p - first) - 1 - i;  // T[p - 1 - i] is character `at` of the window
-        if (at >= 0) chain |= ((window >> (64 - (at + 1) * b)) & mask) << (8 * i);
+        if (at >= 0) chain |= ((window >> (64 - (at + 1) * b)) & mask) << (b * i);
     }
-    return chain;
+    return static_cast<Chain>(chain);
 }
 
 // Element k of text j's class d - 1 with the text's end prepended; keeps p - 1 if it is in class d
-// and in the text, keyed by the code of T[p - 1]. The sort key is the element's chain: the codes of
-// the characters before it, byte 0 first. Pass 1 reads the chains of the sample positions from the
-// code stream (one window each); later passes read the chains the pass before stored in list order,
-// so only pass 1 reads the text at random positions. A text's end reads its own chain every pass.
+// and in the text, keyed by the code of T[p - 1]. The sort key is the element's chain (above).
+// Pass 1 reads the chains of the sample positions from the code stream (one window each); later
+// passes read the chains the pass before stored in list order, so only pass 1 reads the text at
+// random positions. A text's end reads its own chain every pass.
+template <class Chain>
 struct ClassLoader {
+    // 4 tiles per SM (64 registers, some spilled) against 3 (80 registers): the class phase of the
+    // 3 GiB genome-like text took 64.0 ms against 67.9, of the 256 MiB natural text 4.86 against 5.11
+    // (64-bit chains).
+    static constexpr int kTilesPerSm = 4;
     const uint32_t* __restrict__ lists;       // global lists
     const uint32_t* __restrict__ prevOffset;  // rowBase row of class d - 1: text j's slice offset
-    const uint64_t* __restrict__ chains;      // chains of class d - 1 by index from prevStart (d >= 2)
+    const Chain* __restrict__ chains;         // chains of class d - 1 by index from prevStart (d >= 2)
     uint32_t prevStart;                       // first slot of class d - 1 in the global lists
     TextSet texts;
     uint32_t d;
     __device__ __forceinline__ uint32_t element(uint32_t j, uint32_t k) const {
         return k == 0 ? texts.endOfText(j) : lists[__ldg(prevOffset + j) + k - 1];
     }
-    __device__ __forceinline__ bool load(uint32_t j, uint32_t, uint32_t k, uint64_t& key, uint32_t& dig) const {
+    __device__ __forceinline__ bool load(uint32_t j, uint32_t, uint32_t k, Chain& key, uint32_t& dig) const {
         const uint32_t start = texts.startOf(j), end = texts.endOfText(j);
         const uint32_t p = element(j, k);
         // A stored chain is read for every element, kept or not (the reads are sequential), so that
         // it is in flight together with the position instead of waiting for the filter.
         const bool stored = k > 0 && d > 1;
-        const uint64_t chain = stored ? chains[__ldg(prevOffset + j) - prevStart + k - 1] : 0;
+        const Chain chain = stored ? chains[__ldg(prevOffset + j) - prevStart + k - 1] : Chain(0);
         if (p <= start || p > end || classOfResidue((p - 1) % kV) != d) return false;
-        key = stored ? chain : codesBefore(texts, p);
-        dig = static_cast<uint32_t>(key & 0xFF);  // codes order like the bytes they stand for
+        key = stored ? chain : codesBefore<Chain>(texts, p);
+        dig = static_cast<uint32_t>(key) & ((1u << texts.bits) - 1);  // codes order like the bytes they stand for
         return true;
     }
     __device__ __forceinline__ uint32_t value(uint32_t j, uint32_t, uint32_t k) const { return element(j, k) - 1; }
@@ -215,13 +226,15 @@ struct ClassLoader {
 
 // Writes class d's positions, and (unless chains is null: the last class) the chains of its
 // elements: an element p - 1 has p's chain less its first character.
+template <class Chain>
 struct ClassStorer {
     static constexpr bool kKeys = true;
     uint32_t* __restrict__ lists;
-    uint64_t* __restrict__ chains;  // by index from lo
-    uint32_t lo, hi;                // class d's slots in the global lists
-    __device__ __forceinline__ void storeKey(uint32_t, uint32_t pos, uint64_t chain) const {
-        if (chains && pos >= lo && pos < hi) chains[pos - lo] = chain >> 8;
+    Chain* __restrict__ chains;  // by index from lo
+    uint32_t lo, hi;             // class d's slots in the global lists
+    uint32_t bits;
+    __device__ __forceinline__ void storeKey(uint32_t, uint32_t pos, Chain chain) const {
+        if (chains && pos >= lo && pos < hi) chains[pos - lo] = static_cast<Chain>(chain >> bits);
     }
     __device__ __forceinline__ void storeValue(uint32_t, uint32_t pos, uint32_t v) const {
         if (pos >= lo && pos < hi) lists[pos] = v;  // always, unless a look-back timed out
@@ -275,6 +288,27 @@ __global__ void __launch_bounds__(256) classDigitBase(uint32_t* __restrict__ his
     row[threadIdx.x] = rowBase[blockIdx.x] + inclusive - v;
 }
 
+// Passes 1 to kClasses - 1: class d from class d - 1, chains of type Chain in the two chain buffers.
+template <class Chain>
+inline cudaError_t classPasses(const TextSet& texts, const ClassPlan& plan, const ClassTables& tables, uint32_t* lists,
+                               const uint32_t* hist, const RadixScratch& radix, uint64_t* const chains[2],
+                               cudaStream_t stream) {
+    const uint32_t J = tables.texts;
+    for (int d = 1; d < kClasses; d++) {
+        if (plan.start[d + 1] == plan.start[d]) continue;
+        ClassLoader<Chain> ld{lists, tables.rowBase + static_cast<size_t>(d - 1) * J,
+                              reinterpret_cast<const Chain*>(chains[d & 1]), plan.start[d - 1], texts,
+                              static_cast<uint32_t>(d)};
+        ClassStorer<Chain> st{lists, d + 1 < kClasses ? reinterpret_cast<Chain*>(chains[(d + 1) & 1]) : nullptr,
+                              plan.start[d], plan.start[d + 1], texts.bits};
+        ManySegments segs{tables.tileStart + static_cast<size_t>(d) * (J + 1),
+                          tables.elementStart + static_cast<size_t>(d) * (J + 1), J};
+        SADCS_TRY((radixOnesweepPass<Chain, ClassLoader<Chain>, ClassStorer<Chain>, ManySegments>(
+            ld, st, segs, plan.inputs[d], plan.tiles[d], hist + static_cast<size_t>(d) * J * 256, radix, stream)));
+    }
+    return cudaSuccess;
+}
+
 // Fills lists (laid out by plan.start, text-major inside each class) from the sample ranks.
 // tables: the ClassTables block on the device; scratch: classScratchWords(total, J) words.
 // total: bytes of the concatenation (text buffer) scanned by the histogram.
@@ -298,17 +332,13 @@ inline cudaError_t sortClasses(uint32_t total, const TextSet& texts, const uint3
     const uint32_t blocks = std::min<uint32_t>(ceilDiv(total + 7ull, 256 * 8 * 8), 148 * 8);
     SADCS_TRY(launch(classHistogram, std::max(blocks, 1u), 256, 0, stream, total, texts, hist));
     SADCS_TRY(launch(classDigitBase, kClasses * J, 256, 0, stream, hist, tables.rowBase));
-    for (int d = 1; d < kClasses; d++) {
-        if (plan.start[d + 1] == plan.start[d]) continue;
-        ClassLoader ld{lists, tables.rowBase + static_cast<size_t>(d - 1) * J, chains[d & 1], plan.start[d - 1], texts,
-                       static_cast<uint32_t>(d)};
-        ClassStorer st{lists, d + 1 < kClasses ? chains[(d + 1) & 1] : nullptr, plan.start[d], plan.start[d + 1]};
-        ManySegments segs{tables.tileStart + static_cast<size_t>(d) * (J + 1),
-                          tables.elementStart + static_cast<size_t>(d) * (J + 1), J};
-        SADCS_TRY((radixOnesweepPass<uint64_t, ClassLoader, ClassStorer, ManySegments>(
-            ld, st, segs, plan.inputs[d], plan.tiles[d], hist + static_cast<size_t>(d) * J * 256, radix, stream)));
+    if (texts.bits * kChainChars <= 16) {
+        return classPasses<uint16_t>(texts, plan, tables, lists, hist, radix, chains, stream);
     }
-    return cudaSuccess;
+    if (texts.bits * kChainChars <= 32) {
+        return classPasses<uint32_t>(texts, plan, tables, lists, hist, radix, chains, stream);
+    }
+    return classPasses<uint64_t>(texts, plan, tables, lists, hist, radix, chains, stream);
 }
 
 }  // namespace sadcs

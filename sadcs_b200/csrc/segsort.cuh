@@ -5,6 +5,7 @@
 // Most segments are small (on genome-like text every segment left after the first pass has at most
 // 4 members; on natural-language text 80-95% of the remaining suffixes are in segments of up to a
 // few thousand), so:
+//   - segments of up to kSegTiny elements are sorted by one thread each in registers;
 //   - segments of up to kSegSmall elements are sorted entirely in shared memory: a block takes the
 //     segments that start in one kSegChunk-wide range of list positions (at most kSegCap elements)
 //     and radix-sorts them by (segment, subkey) with 8-bit digits, the keys travelling in registers
@@ -29,6 +30,7 @@ namespace sadcs {
 #endif
 
 constexpr uint32_t kSegSmall = SADCS_SEGSORT_SMALL;  // largest segment sorted in one block
+constexpr uint32_t kSegTiny = 8;  // largest segment one thread sorts in registers
 constexpr uint32_t kSegChunk = SADCS_SEGSORT_SMALL;  // a block owns the segments starting in such a range
 constexpr uint32_t kSegCap = kSegChunk + kSegSmall;  // elements a block can hold
 constexpr int kSegThreads = 256;
@@ -137,6 +139,50 @@ __global__ void __launch_bounds__(256) segDigitBase(uint32_t* __restrict__ hist,
     row[threadIdx.x] = begin[blockIdx.x] + inclusive - v;
 }
 
+// Segments of 2 to kSegTiny elements, one thread each: keys and values into registers, sorted
+// by compare-exchange at fixed register indices (an insertion sort unrolled for kSegTiny), written
+// back in place. On genome-like text most groups left after the first pass are a repeat and its
+// copies (2-4 members), which the block-wide radix sort would take 4 to 8 passes over.
+__global__ void __launch_bounds__(256) segSortTiny(const uint32_t* __restrict__ heads, uint32_t segments,
+                                                   uint64_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= segments) return;
+    const uint32_t begin = heads[k], size = heads[k + 1] - begin;
+    if (size < 2 || size > kSegTiny) return;
+    uint64_t key[kSegTiny];
+    uint32_t val[kSegTiny];
+#pragma unroll
+    for (uint32_t i = 0; i < kSegTiny; i++) {
+        if (i < size) {
+            key[i] = keys[begin + i];
+            val[i] = vals[begin + i];
+        }
+    }
+#pragma unroll
+    for (uint32_t i = 1; i < kSegTiny; i++) {
+        if (i < size) {
+#pragma unroll
+            for (uint32_t j = i; j > 0; j--) {
+                if (key[j - 1] > key[j]) {
+                    const uint64_t tk = key[j - 1];
+                    key[j - 1] = key[j];
+                    key[j] = tk;
+                    const uint32_t tv = val[j - 1];
+                    val[j - 1] = val[j];
+                    val[j] = tv;
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (uint32_t i = 0; i < kSegTiny; i++) {
+        if (i < size) {
+            keys[begin + i] = key[i];
+            vals[begin + i] = val[i];
+        }
+    }
+}
+
 // Copies the big segments' ranges from one buffer pair to the other.
 __global__ void segCopyBack(ListSegments segs, const uint64_t* __restrict__ kFrom, const uint32_t* __restrict__ vFrom,
                             uint64_t* __restrict__ kTo, uint32_t* __restrict__ vTo) {
@@ -190,7 +236,7 @@ __global__ void __launch_bounds__(kSegThreads, SADCS_SEGSORT_BLOCKS) segSortSmal
         uint32_t size = 0;
         if (s < count) {
             const uint32_t start = heads[first + s], end = heads[first + s + 1];
-            size = end - start <= kSegSmall ? end - start : 0;
+            size = end - start <= kSegSmall && end - start > kSegTiny ? end - start : 0;  // tiny ones: segSortTiny
             segStart[s] = start;
         }
         uint32_t total;
@@ -352,6 +398,7 @@ inline cudaError_t segmentedSort(const uint32_t* grp, uint32_t u, uint64_t* keys
         return cudaFuncSetAttribute(segSortSmall, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     static_cast<int>(segSortSharedBytes()));
     }));
+    SADCS_TRY(launch(segSortTiny, ceilDiv(segments, 256), 256, 0, stream, b.heads, segments, keys, vals));
     SADCS_TRY(launch(segSortSmall, ceilDiv(u, kSegChunk), kSegThreads, segSortSharedBytes(), stream, b.heads,
                      segments, keys, vals, keys, vals, keyBits));
     if (big == 0) return cudaSuccess;

@@ -9,7 +9,8 @@
 // the constructions already admitted. Each worker has its own stream and takes its slab from a
 // stream-ordered memory pool, so constructions of different workers overlap on the device (the
 // radix look-back backs off while it waits, so that waiting tiles do not slow the constructions
-// beside them: 3 workers give 1.2x the throughput of 1 on the served mix).
+// beside them: 3 workers give 1.2x the throughput of 1 on the served mix). With two workers or
+// more, worker 0 is a small-request lane (server_policy.h): large requests never hold every worker.
 // A request's outputs are exactly those of a construction of its text alone.
 #pragma once
 
@@ -60,6 +61,7 @@ struct sadcs_gpu_server {
     uint64_t smallLimit = 0;   // requests up to this many bytes may share a batch
     uint64_t batchBytes = 0;   // bytes of text per batch
     uint32_t batchTexts = 0;   // texts per batch
+    int workers = 0;           // worker threads (set before they start)
     uint64_t nextId = 1;
     bool stopping = false;
     cudaMemPool_t pool = nullptr;
@@ -186,8 +188,9 @@ void serveBatch(sadcs_gpu_server* srv, sadcs_gpu_context& ctx, std::vector<Serve
     srv->work.notify_all();
 }
 
-void serverWorker(sadcs_gpu_server* srv) {
+void serverWorker(sadcs_gpu_server* srv, int worker) {
     cudaSetDevice(srv->device);
+    const bool smallLane = serverIsSmallLane(worker, srv->workers);
     sadcs_gpu_context ctx;
     ctx.device = srv->device;
     ctx.hostWordCount = 64 + metaWords(srv->batchTexts, 0) + 2 * static_cast<size_t>(srv->batchTexts) + 64 + 256;
@@ -202,22 +205,23 @@ void serverWorker(sadcs_gpu_server* srv) {
             std::unique_lock<std::mutex> lock(srv->mu);
             for (;;) {
                 if (srv->stopping && srv->queue.empty()) break;
-                if (!srv->queue.empty()) {
-                    // Take the head alone (large) or the queued small requests that fit one batch
-                    // (server_policy.h).
+                // The group's first request: the head, or for the small lane the first small one.
+                const size_t first = serverGroupStart(
+                    srv->queue.size(), [srv](size_t k) { return srv->queue[k]->n; }, srv->smallLimit, smallLane);
+                if (first < srv->queue.size()) {
+                    // Take that request alone (large) or it and the queued small requests after it
+                    // that fit one batch (server_policy.h).
                     const size_t take = serverGroupSize(
-                        srv->queue.size(), [srv](size_t k) { return srv->queue[k]->n; }, srv->smallLimit,
-                        srv->batchBytes, srv->batchTexts);
+                        srv->queue.size() - first, [srv, first](size_t k) { return srv->queue[first + k]->n; },
+                        srv->smallLimit, srv->batchBytes, srv->batchTexts);
                     std::vector<uint64_t> lengths(take);
-                    for (size_t k = 0; k < take; k++) lengths[k] = srv->queue[k]->n;
+                    for (size_t k = 0; k < take; k++) lengths[k] = srv->queue[first + k]->n;
                     Batch candidate;
                     planBatch(lengths.data(), static_cast<uint32_t>(lengths.size()), candidate);
                     const size_t need = footprintOf(candidate);
                     if (serverAdmits(need, srv->inUse, srv->budget)) {
-                        for (size_t k = 0; k < take; k++) {
-                            group.push_back(srv->queue.front());
-                            srv->queue.pop_front();
-                        }
+                        for (size_t k = 0; k < take; k++) group.push_back(srv->queue[first + k]);
+                        srv->queue.erase(srv->queue.begin() + first, srv->queue.begin() + first + take);
                         b = std::move(candidate);
                         footprint = need;
                         srv->inUse += need;
@@ -300,7 +304,8 @@ int sadcs_gpu_server_create(int64_t memory_budget, int32_t workers, int64_t smal
         delete srv;
         return status;
     }
-    for (int32_t w = 0; w < workers; w++) srv->threads.emplace_back(serverWorker, srv);
+    srv->workers = workers;
+    for (int32_t w = 0; w < workers; w++) srv->threads.emplace_back(serverWorker, srv, w);
     *out = srv;
     return SADCS_OK;
 }

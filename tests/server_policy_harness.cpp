@@ -14,3 +14,11 @@ extern "C" size_t policy_group_size(const uint64_t* lengths, size_t count, uint6
 extern "C" int policy_admits(uint64_t need, uint64_t in_use, uint64_t budget) {
     return sadcs::serverAdmits(need, in_use, budget) ? 1 : 0;
 }
+
+extern "C" size_t policy_group_start(const uint64_t* lengths, size_t count, uint64_t small_limit, int small_lane) {
+    return sadcs::serverGroupStart(count, [lengths](size_t k) { return lengths[k]; }, small_limit, small_lane != 0);
+}
+
+extern "C" int policy_is_small_lane(int worker, int workers) {
+    return sadcs::serverIsSmallLane(worker, workers) ? 1 : 0;
+}

@@ -92,3 +92,32 @@ def test_admission():
     assert admits(5, 5, 10)  # fits beside the running ones (inclusive)
     assert not admits(6, 5, 10)
     assert not admits(1, 10, 10)
+
+
+def test_small_lane_starts_at_the_first_small_request():
+    """Worker 0 of two or more is the small lane: its group starts at the first small request of the
+    queue (large ones ahead of it are left to the other workers); the others start at the head."""
+    L = policy()
+    L.policy_group_start.restype = ctypes.c_size_t
+    L.policy_group_start.argtypes = [ctypes.POINTER(ctypes.c_uint64), ctypes.c_size_t, ctypes.c_uint64, ctypes.c_int]
+
+    def start(lengths, small_limit, lane):
+        a = np.ascontiguousarray(lengths, dtype=np.uint64)
+        keep = a if len(a) else np.zeros(1, np.uint64)
+        return L.policy_group_start(keep.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), len(a), small_limit, lane)
+
+    assert start([5000, 6000, 10, 20], 100, 1) == 2
+    assert start([5000, 6000, 10, 20], 100, 0) == 0
+    assert start([5000, 6000], 100, 1) == 2  # nothing small: the lane waits
+    assert start([], 100, 1) == 0
+    assert start([10, 5000], 100, 1) == 0
+    assert [L.policy_is_small_lane(w, n) for n in (1, 2, 3) for w in range(n)] == [0, 1, 0, 1, 0, 0]
+    rng = np.random.default_rng(9)
+    for _ in range(500):
+        lengths = [int(x) for x in rng.choice([10, 50, 90, 1000, 5000], size=int(rng.integers(0, 12)))]
+        got = start(lengths, 100, 1)
+        expected = next((k for k, n in enumerate(lengths) if n <= 100), len(lengths))
+        assert got == expected
+        # the lane's group is the grouping rule applied from there on
+        if got < len(lengths):
+            assert group_size(lengths[got:], 100, 400, 3) == stated_rule(lengths[got:], 100, 400, 3)
