@@ -26,7 +26,9 @@ ranks itself (torch.distributed.run on this node).
 Beside the line's own figures: ``cpu_baseline`` (the reference's CPU build on a prefix sample, the
 same sample as the --impl reference arm) and, on one GPU, ``reference_gpu`` (the reference's own
 CUDA build on this GPU, on the largest prefix its int32 API takes, SA then BWT, next to this
-library's construction of the same prefix).
+library's construction of the same prefix) and ``batch`` (the batch4096 workload: one batched
+construction of 4096 uneven texts against one construction per text on a sample of them, whose
+outputs are checked equal).
 """
 from __future__ import annotations
 
@@ -495,9 +497,11 @@ def run_ours(args, world, rank, local) -> None:
                 "kernel_ms": round(merge_avg, 3), "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"}
     traffic = profile_traffic(args.workload)
     if traffic:
-        roofline["traffic"] = round(traffic * n)
-        roofline["traffic_source"] = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the final merge on this "
-                                      "workload, per input byte (profiles/traffic.json), times n")
+        roofline["traffic"] = round(traffic[0] * n)
+        roofline["traffic_source"] = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the final merge per input "
+                                      "byte, captured on %s (profiles/traffic.json), times n%s" % (
+                                          traffic[1], "" if traffic[1] == args.workload else
+                                          ": scaled to this size, a lower bound (less of the gathers hit L2)"))
     line = {"metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms_max, 3), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u8", "data": "synthetic",
@@ -606,11 +610,12 @@ def verify_on_device(d_text, d_sa, d_bwt, primary) -> bool:
 
 
 def profile_traffic(workload: str):
-    """DRAM bytes per input byte of the final merge kernel, from the committed ncu summary."""
+    """(DRAM bytes per input byte of the final merge kernel, the workload they were captured on),
+    from the committed ncu summary (profiles/traffic.json), or None."""
     path = ROOT / "profiles" / "traffic.json"
     try:
-        data = json.loads(path.read_text())
-        return float(data[workload]["merge_dram_bytes_per_input_byte"])
+        entry = json.loads(path.read_text())[workload]
+        return float(entry["merge_dram_bytes_per_input_byte"]), entry.get("scaled_from", workload)
     except Exception:
         return None
 
