@@ -10,7 +10,8 @@
 // stream-ordered memory pool, so constructions of different workers overlap on the device (the
 // radix look-back backs off while it waits, so that waiting tiles do not slow the constructions
 // beside them: 3 workers give 1.2x the throughput of 1 on the served mix). With two workers or
-// more, worker 0 is a small-request lane (server_policy.h): large requests never hold every worker.
+// more, worker 0 is a small-request lane (server_policy.h): large requests never hold every worker,
+// and its stream has the highest priority, so its kernels do not wait behind a large construction's.
 // A request's outputs are exactly those of a construction of its text alone.
 #pragma once
 
@@ -194,7 +195,13 @@ void serverWorker(sadcs_gpu_server* srv, int worker) {
     sadcs_gpu_context ctx;
     ctx.device = srv->device;
     ctx.hostWordCount = 64 + metaWords(srv->batchTexts, 0) + 2 * static_cast<size_t>(srv->batchTexts) + 64 + 256;
-    bool ready = cudaStreamCreateWithFlags(&ctx.stream, cudaStreamNonBlocking) == cudaSuccess &&
+    // The small lane's stream has the device's highest priority: its kernels' blocks are dispatched
+    // first as SMs free up, instead of queueing behind a large construction's grids.
+    int leastPriority = 0, greatestPriority = 0;
+    if (!smallLane || cudaDeviceGetStreamPriorityRange(&leastPriority, &greatestPriority) != cudaSuccess) {
+        greatestPriority = 0;
+    }
+    bool ready = cudaStreamCreateWithPriority(&ctx.stream, cudaStreamNonBlocking, greatestPriority) == cudaSuccess &&
                  cudaMallocHost(&ctx.hostWords, 4 * ctx.hostWordCount) == cudaSuccess;
     for (cudaEvent_t& e : ctx.events) ready = ready && cudaEventCreate(&e) == cudaSuccess;
     for (;;) {

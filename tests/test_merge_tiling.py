@@ -150,52 +150,3 @@ def test_tiles_with_empty_and_tiny_lists():
         for R in (40, 80):
             check_tiling(lists, R)
 
-
-def warp_merge_steps(A, B, d_begin, d_end):
-    """Outputs [d_begin, d_end) of merging sorted A and B, as merge_final.cuh's warpLevel makes them:
-    the merge path's split at d_begin by binary search, then steps of 32 outputs in which lane l
-    holds A[i + l] and B[j + 31 - l] (None past an end: after everything), the smaller of each pair
-    are the 32 smallest (bitonic half-cleaner), five exchange stages sort them, and A's share is the
-    count of lanes whose A element was the smaller (a last, shorter step: A's candidates not after its
-    last output)."""
-    def less(a, b):
-        return a is not None and (b is None or a < b)
-
-    lo, hi = max(0, d_begin - len(B)), min(d_begin, len(A))
-    while lo < hi:
-        mid = (lo + hi) // 2
-        if A[mid] < B[d_begin - 1 - mid]:
-            lo = mid + 1
-        else:
-            hi = mid
-    i, j, d, out = lo, d_begin - lo, d_begin, []
-    while d < d_end:
-        x = [A[i + l] if i + l < len(A) else None for l in range(32)]
-        y = [B[j + 31 - l] if j + 31 - l < len(B) else None for l in range(32)]
-        h = [x[l] if less(x[l], y[l]) else y[l] for l in range(32)]
-        taken_a = sum(less(x[l], y[l]) for l in range(32))
-        k = 16
-        while k:
-            o = [h[l ^ k] for l in range(32)]
-            h = [h[l] if ((l & k) == 0) == less(h[l], o[l]) else o[l] for l in range(32)]
-            k //= 2
-        count = min(32, d_end - d)
-        out += h[:count]
-        if count < 32:
-            taken_a = sum(x[l] is not None and not less(h[count - 1], x[l]) for l in range(32))
-        i, j, d = i + taken_a, j + count - taken_a, d + count
-    return out
-
-
-def test_warp_merge_steps_give_the_merge():
-    rng = np.random.default_rng(21)
-    for _ in range(300):
-        la, lb = (int(v) for v in rng.integers(0, 160, 2))
-        keys = rng.choice(1 << 20, la + lb, replace=False)  # suffixes never compare equal
-        A, B = sorted(keys[:la].tolist()), sorted(keys[la:].tolist())
-        merged = sorted(A + B)
-        cuts = sorted({0, len(merged), *rng.integers(0, len(merged) + 1, 3).tolist()})
-        got = []
-        for a, b in zip(cuts[:-1], cuts[1:]):
-            got += warp_merge_steps(A, B, a, b)
-        assert got == merged
