@@ -108,9 +108,7 @@ inline uint32_t* classErrorWord(uint32_t* scratch, uint32_t texts) {
 // the slice; one run per slice and block); classScatterPairs then walks the pairs slice by slice,
 // and each slice's writes stay within the list's L2-sized slice.
 constexpr uint32_t kSampleSliceShift = 23;  // 8M ranks = 32 MB of the list per slice
-constexpr uint32_t kMaxSampleSlices = 128;
-constexpr int kPartitionThreads = 256;
-constexpr int kPartitionItems = 8;
+constexpr uint32_t kMaxSampleSlices = kMaxSlices;
 
 // The slice width (as a shift) for `live` samples: at least 8M ranks, at most kMaxSampleSlices slices.
 inline uint32_t sampleSliceShift(uint64_t live) {
@@ -120,43 +118,25 @@ inline uint32_t sampleSliceShift(uint64_t live) {
 }
 
 // fill[k] (zeroed by the caller) counts the pairs placed in slice k so far.
-__global__ void __launch_bounds__(kPartitionThreads) classPartitionSample(const uint32_t* __restrict__ ranks,
-                                                                         uint32_t slots, uint32_t live,
-                                                                         uint32_t shift, TextSet texts,
-                                                                         uint32_t* __restrict__ fill,
-                                                                         uint64_t* __restrict__ pairs) {
-    __shared__ uint32_t count[kMaxSampleSlices];
-    __shared__ uint32_t base[kMaxSampleSlices];
-    for (uint32_t i = threadIdx.x; i < kMaxSampleSlices; i += kPartitionThreads) count[i] = 0;
-    __syncthreads();
-    uint32_t r[kPartitionItems], p[kPartitionItems], local[kPartitionItems];
-    const uint64_t first = static_cast<uint64_t>(blockIdx.x) * kPartitionThreads * kPartitionItems + threadIdx.x;
+__global__ void __launch_bounds__(kSliceThreads) classPartitionSample(const uint32_t* __restrict__ ranks,
+                                                                     uint32_t slots, uint32_t live, uint32_t shift,
+                                                                     TextSet texts, uint32_t* __restrict__ fill,
+                                                                     uint64_t* __restrict__ pairs) {
+    __shared__ SliceStage stage;
+    uint64_t v[kSliceItems];
+    const uint64_t first = static_cast<uint64_t>(blockIdx.x) * kSliceTile + threadIdx.x;
 #pragma unroll
-    for (int j = 0; j < kPartitionItems; j++) {
-        const uint64_t t = first + static_cast<uint64_t>(j) * kPartitionThreads;
-        r[j] = 0xFFFFFFFFu;
+    for (int j = 0; j < kSliceItems; j++) {
+        const uint64_t t = first + static_cast<uint64_t>(j) * kSliceThreads;
+        v[j] = kNoPair;
         if (t < slots) {
             const uint32_t rank = __ldcs(ranks + t);  // streamed: read once
             const uint32_t q = samplePosition(static_cast<uint32_t>(t));
-            if (q < texts.endOf(q) && rank < live) {  // a live sample (not past the end or between texts)
-                r[j] = rank;
-                p[j] = q;
-                local[j] = atomicAdd(&count[rank >> shift], 1u);
-            }
+            // a live sample (not past the end or between texts)
+            if (q < texts.endOf(q) && rank < live) v[j] = (static_cast<uint64_t>(rank) << 32) | q;
         }
     }
-    __syncthreads();
-    for (uint32_t k = threadIdx.x; k < kMaxSampleSlices; k += kPartitionThreads) {
-        if (count[k]) base[k] = atomicAdd(fill + k, count[k]);
-    }
-    __syncthreads();
-#pragma unroll
-    for (int j = 0; j < kPartitionItems; j++) {
-        if (r[j] == 0xFFFFFFFFu) continue;
-        const uint32_t k = r[j] >> shift;
-        const uint64_t at = (static_cast<uint64_t>(k) << shift) + base[k] + local[j];
-        if (at < live) pairs[at] = (static_cast<uint64_t>(r[j]) << 32) | p[j];  // always, for a permutation
-    }
+    writeSliceMajor(stage, v, shift, fill, pairs, live);
 }
 
 __global__ void classScatterPairs(const uint64_t* __restrict__ pairs, uint32_t live, uint32_t* __restrict__ list) {
@@ -324,8 +304,8 @@ inline cudaError_t sortClasses(uint32_t total, const TextSet& texts, const uint3
     // (the radix scratch's digit-base words, unused by the class passes).
     uint32_t* fill = radix.digitBase;
     SADCS_TRY(cudaMemsetAsync(fill, 0, kMaxSampleSlices * sizeof(uint32_t), stream));
-    SADCS_TRY(launch(classPartitionSample, ceilDiv(slots, kPartitionThreads * kPartitionItems), kPartitionThreads, 0,
-                     stream, ranks, slots, live, sampleSliceShift(live), texts, fill, chains[0]));
+    SADCS_TRY(launch(classPartitionSample, ceilDiv(slots, kSliceTile), kSliceThreads, 0, stream, ranks, slots, live,
+                     sampleSliceShift(live), texts, fill, chains[0]));
     SADCS_TRY(launch(classScatterPairs, ceilDiv(live, 256), 256, 0, stream, chains[0], live, lists));
     SADCS_TRY(cudaMemsetAsync(hist, 0, static_cast<size_t>(kClasses) * J * 256 * 4, stream));
     SADCS_TRY(cudaMemsetAsync(radix.control, 0, 8, stream));

@@ -157,6 +157,82 @@ cudaError_t deviceScan(const uint32_t* in, uint32_t* out, uint32_t count, uint32
     return cudaGetLastError();
 }
 
+// ---- partition of 64-bit pairs into slices -------------------------------------------------------
+//
+// The two-level scatters (the class-0 list, the rank writes of large ranking passes) first move
+// (index, value) pairs, index in the high word, into the slice of the target array their index
+// belongs to: slice k of the pair array is [k << shift, (k + 1) << shift) and receives the pairs
+// whose index lies in the target's slice k (at most 2^shift, one per index). A block stages its
+// tile of pairs slice by slice in shared memory, reserves each slice's run with one atomic, and
+// writes the runs with consecutive threads on consecutive words, so the pair array is written in
+// whole sectors rather than by scattered 8-byte stores.
+constexpr int kSliceThreads = 256;
+constexpr int kSliceItems = 16;
+constexpr uint32_t kSliceTile = kSliceThreads * kSliceItems;
+constexpr uint32_t kMaxSlices = 128;
+constexpr uint64_t kNoPair = ~uint64_t(0);
+
+struct SliceStage {
+    uint32_t count[kMaxSlices];
+    uint32_t offset[kMaxSlices];
+    uint32_t base[kMaxSlices];
+    uint64_t pairs[kSliceTile];
+};
+
+// All threads of the block, each with its kSliceItems pairs (kNoPair where it has none, and for
+// any pair whose slice is not below kMaxSlices). fill[k] (zeroed by the caller before the launch)
+// counts the pairs placed in slice k; capacity bounds the pair array.
+__device__ __forceinline__ void writeSliceMajor(SliceStage& st, const uint64_t (&v)[kSliceItems], uint32_t shift,
+                                                uint32_t* __restrict__ fill, uint64_t* __restrict__ dst,
+                                                uint64_t capacity) {
+    for (uint32_t i = threadIdx.x; i < kMaxSlices; i += kSliceThreads) st.count[i] = 0;
+    __syncthreads();
+    uint32_t local[kSliceItems];
+#pragma unroll
+    for (int j = 0; j < kSliceItems; j++) {
+        local[j] = v[j] == kNoPair ? 0 : atomicAdd(&st.count[static_cast<uint32_t>(v[j] >> 32) >> shift], 1u);
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {  // exclusive scan of the counts, 4 slices per lane
+        const uint32_t lane = threadIdx.x;
+        uint32_t c[4], sum = 0;
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            c[q] = st.count[4 * lane + q];
+            sum += c[q];
+        }
+        uint32_t inclusive = sum;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t up = __shfl_up_sync(0xffffffffu, inclusive, d);
+            if (lane >= static_cast<uint32_t>(d)) inclusive += up;
+        }
+        uint32_t at = inclusive - sum;
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            st.offset[4 * lane + q] = at;
+            at += c[q];
+        }
+    }
+    if (threadIdx.x < kMaxSlices && st.count[threadIdx.x]) {
+        st.base[threadIdx.x] = atomicAdd(fill + threadIdx.x, st.count[threadIdx.x]);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < kSliceItems; j++) {
+        if (v[j] != kNoPair) st.pairs[st.offset[static_cast<uint32_t>(v[j] >> 32) >> shift] + local[j]] = v[j];
+    }
+    __syncthreads();
+    const uint32_t total = st.offset[kMaxSlices - 1] + st.count[kMaxSlices - 1];
+    for (uint32_t i = threadIdx.x; i < total; i += kSliceThreads) {
+        const uint64_t pair = st.pairs[i];
+        const uint32_t k = static_cast<uint32_t>(pair >> 32) >> shift;
+        const uint32_t rel = st.base[k] + (i - st.offset[k]);
+        const uint64_t at = (static_cast<uint64_t>(k) << shift) + rel;
+        if ((static_cast<uint64_t>(rel) >> shift) == 0 && at < capacity) dst[at] = pair;  // always, by construction
+    }
+}
+
 // ---- radix pass (onesweep) ------------------------------------------------------------------
 //
 // One stable counting pass on an 8-bit digit per kernel, reading and writing each element once

@@ -342,7 +342,7 @@ __global__ void __launch_bounds__(kRefineThreads) rankRefineApply(const uint32_t
 // and rankScatterPairs writes the slices one after another, each within an L2-sized part of the
 // rank array.
 constexpr uint32_t kRankSliceShift = 23;  // 8M samples = 32 MB of the rank array per slice
-constexpr uint32_t kMaxRankSlices = 128;
+constexpr uint32_t kMaxRankSlices = kMaxSlices;
 constexpr int kPairThreads = 256;
 constexpr int kPairItems = 8;
 constexpr uint32_t kPairTile = kPairThreads * kPairItems;  // divides 2^kRankSliceShift
@@ -355,44 +355,25 @@ inline uint32_t rankSliceShift(uint64_t slots) {
     return shift;
 }
 
-// pairs[0, count) -> dst, slice-major; count = u (every element wrote) or u less the kept total.
-// fill[k] (zeroed by the caller) counts the pairs placed in slice k.
-__global__ void __launch_bounds__(kPairThreads) rankPartitionPairs(const uint64_t* __restrict__ pairs, uint32_t u,
-                                                                   const uint32_t* __restrict__ keptTotal,
-                                                                   uint32_t writeAll, uint32_t shift,
-                                                                   uint32_t capacity, uint32_t* __restrict__ fill,
-                                                                   uint64_t* __restrict__ dst) {
-    __shared__ uint32_t count[kMaxRankSlices];
-    __shared__ uint32_t base[kMaxRankSlices];
-    for (uint32_t i = threadIdx.x; i < kMaxRankSlices; i += kPairThreads) count[i] = 0;
-    __syncthreads();
+// pairs[0, count) -> dst, slice-major (writeSliceMajor); count = u (every element wrote) or u less
+// the kept total. fill[k] (zeroed by the caller) counts the pairs placed in slice k.
+__global__ void __launch_bounds__(kSliceThreads) rankPartitionPairs(const uint64_t* __restrict__ pairs, uint32_t u,
+                                                                    const uint32_t* __restrict__ keptTotal,
+                                                                    uint32_t writeAll, uint32_t shift,
+                                                                    uint32_t capacity, uint32_t* __restrict__ fill,
+                                                                    uint64_t* __restrict__ dst) {
+    __shared__ SliceStage stage;
     const uint32_t total = writeAll ? u : u - min(*keptTotal, u);
-    uint64_t v[kPairItems];
-    uint32_t local[kPairItems];
-    const uint64_t first = static_cast<uint64_t>(blockIdx.x) * kPairTile + threadIdx.x;
+    uint64_t v[kSliceItems];
+    const uint64_t first = static_cast<uint64_t>(blockIdx.x) * kSliceTile + threadIdx.x;
 #pragma unroll
-    for (int j = 0; j < kPairItems; j++) {
-        const uint64_t i = first + static_cast<uint64_t>(j) * kPairThreads;
-        v[j] = i < total ? __ldcs(pairs + i) : ~uint64_t(0);
-        const uint32_t t = static_cast<uint32_t>(v[j] >> 32);
-        if ((t >> shift) < kMaxRankSlices) {
-            local[j] = atomicAdd(&count[t >> shift], 1u);
-        } else {
-            v[j] = ~uint64_t(0);  // no pair, or a guarded out-of-range sample
-        }
+    for (int j = 0; j < kSliceItems; j++) {
+        const uint64_t i = first + static_cast<uint64_t>(j) * kSliceThreads;
+        v[j] = i < total ? __ldcs(pairs + i) : kNoPair;
+        // no pair, or a guarded out-of-range sample
+        if ((static_cast<uint32_t>(v[j] >> 32) >> shift) >= kMaxRankSlices) v[j] = kNoPair;
     }
-    __syncthreads();
-    for (uint32_t k = threadIdx.x; k < kMaxRankSlices; k += kPairThreads) {
-        if (count[k]) base[k] = atomicAdd(fill + k, count[k]);
-    }
-    __syncthreads();
-#pragma unroll
-    for (int j = 0; j < kPairItems; j++) {
-        if (v[j] == ~uint64_t(0)) continue;
-        const uint32_t k = static_cast<uint32_t>(v[j] >> 32) >> shift;
-        const uint64_t at = (static_cast<uint64_t>(k) << shift) + base[k] + local[j];
-        if (at < capacity && base[k] + local[j] < (1u << shift)) dst[at] = v[j];  // always, by construction
-    }
+    writeSliceMajor(stage, v, shift, fill, dst, capacity);
 }
 
 // Block b writes the pairs of dst[b * kPairTile, (b + 1) * kPairTile) that its slice holds.
@@ -433,6 +414,9 @@ inline int bitWidth(uint64_t x) {
 // 256 MiB natural-language-like text (6-bit codes) 6 characters in 5 passes left more suffixes in
 // word-sized repeats for the later passes (17.5 to 19.2 ms).
 constexpr uint32_t kMinFirstPassChars = 16;
+#ifndef SADCS_FIRST_PASS_MARGIN_BITS
+#define SADCS_FIRST_PASS_MARGIN_BITS 6  // 2^(chars * bits) >= 2^6 x samples (tuning)
+#endif
 inline uint32_t firstPassChars(const TextSet& texts, uint64_t samples) {
     auto width = [](uint32_t x) {
         uint32_t w = 0;
@@ -443,7 +427,7 @@ inline uint32_t firstPassChars(const TextSet& texts, uint64_t samples) {
         return w;
     };
     const uint32_t b = texts.bits;
-    const uint32_t wantBits = static_cast<uint32_t>(bitWidth(samples)) + 6;
+    const uint32_t wantBits = static_cast<uint32_t>(bitWidth(samples)) + SADCS_FIRST_PASS_MARGIN_BITS;
     for (uint32_t passes = 1; passes <= 8; passes++) {
         uint32_t c = std::min<uint32_t>(texts.keyChars, (8 * passes) / b);
         while (c > 0 && c * b + width(c) > 8 * passes) c--;
@@ -527,8 +511,8 @@ inline cudaError_t rankSample(const uint8_t* text, const TextSet& texts, uint32_
             const uint32_t shift = rankSliceShift(slots);
             uint32_t* fill = b.scratch;  // the first sort's digit bases, dead after it
             SADCS_TRY(cudaMemsetAsync(fill, 0, kMaxRankSlices * sizeof(uint32_t), stream));
-            SADCS_TRY(launch(rankPartitionPairs, ceilDiv(u, kPairTile), kPairThreads, 0, stream, keyAlt, u, b.counter,
-                             writeAll ? 1u : 0u, shift, b.keyEntries, fill, key));
+            SADCS_TRY(launch(rankPartitionPairs, ceilDiv(u, kSliceTile), kSliceThreads, 0, stream, keyAlt, u,
+                             b.counter, writeAll ? 1u : 0u, shift, b.keyEntries, fill, key));
             SADCS_TRY(launch(rankScatterPairs, ceilDiv(slots, kPairTile), kPairThreads, 0, stream, key, shift,
                              b.keyEntries, slots, fill, ranks));
         }
