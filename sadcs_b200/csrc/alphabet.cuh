@@ -53,26 +53,61 @@ __global__ void __launch_bounds__(256) alphabetHistogram(const uint8_t* __restri
     if (sum) atomicAdd(counts + threadIdx.x, sum);
 }
 
-// packed[w] = the 64 bits [64w, 64w + 64) of the code stream. One thread per word; positions past
-// the end of the concatenation read code 0. The byte-to-code table is copied to shared memory
-// first: indexed by data, a kernel-parameter table would serialise a warp's lookups.
+// The code stream in groups: a group of G = 64 / gcd(bits, 64) characters fills exactly
+// G * bits / 64 whole words (DNA: 32 characters, one word; 6-bit codes: 32 characters, three words),
+// so one thread packs a group from its bytes read by 16-byte loads (8-byte for 8-bit codes) and
+// writes its words. Positions past the end of the concatenation read code 0. The byte-to-code table
+// is copied to shared memory first: indexed by data, a kernel-parameter table would serialise a
+// warp's lookups.
+__host__ __device__ constexpr uint32_t packGroupChars(uint32_t bits) {
+    return 64u / (bits & (0u - bits));  // gcd(bits, 64): the lowest set bit of bits (bits <= 8)
+}
+
 __global__ void __launch_bounds__(256) packCodes(const uint8_t* __restrict__ text, uint32_t total, CodeTable table,
                                                  uint32_t bits, uint64_t words, uint64_t* __restrict__ packed) {
     __shared__ uint8_t code[256];
     code[threadIdx.x] = table.code[threadIdx.x];
     __syncthreads();
-    const uint64_t w = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (w >= words) return;
-    const uint64_t firstBit = w * 64;
-    const uint64_t first = firstBit / bits, last = (firstBit + 63) / bits;
-    uint64_t out = 0;
-    for (uint64_t q = first; q <= last; q++) {
-        const uint64_t c = q < total ? code[text[q]] : 0;
-        // character q spans stream bits [q*bits, q*bits + bits); place it relative to this word
-        const int64_t shift = static_cast<int64_t>(firstBit + 64) - static_cast<int64_t>(q * bits + bits);
-        out |= shift >= 0 ? (shift < 64 ? c << shift : 0) : c >> (-shift);
+    const uint32_t G = packGroupChars(bits), perGroup = G * bits / 64;
+    const uint64_t group = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const uint64_t firstWord = group * perGroup;
+    if (firstWord >= words) return;
+    const uint64_t firstChar = group * G;
+    uint64_t acc = 0, out = firstWord;
+    uint32_t filled = 0;
+    auto put = [&](uint32_t c) {
+        if (filled + bits <= 64) {
+            acc = (acc << bits) | c;
+            filled += bits;
+            if (filled == 64) {
+                if (out < words) packed[out] = acc;
+                out++;
+                acc = 0;
+                filled = 0;
+            }
+        } else {  // the character straddles two words
+            const uint32_t over = filled + bits - 64;
+            if (out < words) packed[out] = (acc << (bits - over)) | (c >> over);
+            out++;
+            acc = c & ((1u << over) - 1);
+            filled = over;
+        }
+    };
+    const uint32_t step = G >= 16 ? 16 : 8;
+    for (uint32_t piece = 0; piece < G; piece += step) {
+        const uint64_t q0 = firstChar + piece;
+        uint8_t bytes[16];
+        if (q0 + step <= total) {  // inside the text: one aligned vector load
+            if (step == 16) {
+                *reinterpret_cast<uint4*>(bytes) = *reinterpret_cast<const uint4*>(text + q0);
+            } else {
+                *reinterpret_cast<uint2*>(bytes) = *reinterpret_cast<const uint2*>(text + q0);
+            }
+        } else {
+            for (uint32_t k = 0; k < step; k++) bytes[k] = q0 + k < total ? text[q0 + k] : 0;
+        }
+        for (uint32_t k = 0; k < step; k++) put(q0 + k < total ? code[bytes[k]] : 0u);
     }
-    packed[w] = out;
 }
 
 // 64 bits of the code stream starting at stream bit `bit`.

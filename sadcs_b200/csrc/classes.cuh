@@ -174,12 +174,16 @@ __device__ __forceinline__ Chain codesBefore(const TextSet& texts, uint32_t p) {
 // Pass 1 reads the chains of the sample positions from the code stream (one window each); later
 // passes read the chains the pass before stored in list order, so only pass 1 reads the text at
 // random positions. A text's end reads its own chain every pass.
+#ifndef SADCS_CLASS_TILES
+#define SADCS_CLASS_TILES 4  // onesweep tiles per SM of the class passes (tuning)
+#endif
+
 template <class Chain>
 struct ClassLoader {
     // 4 tiles per SM (64 registers, some spilled) against 3 (80 registers): the class phase of the
     // 3 GiB genome-like text took 64.0 ms against 67.9, of the 256 MiB natural text 4.86 against 5.11
     // (64-bit chains).
-    static constexpr int kTilesPerSm = 4;
+    static constexpr int kTilesPerSm = SADCS_CLASS_TILES;
     const uint32_t* __restrict__ lists;       // global lists
     const uint32_t* __restrict__ prevOffset;  // rowBase row of class d - 1: text j's slice offset
     const Chain* __restrict__ chains;         // chains of class d - 1 by index from prevStart (d >= 2)

@@ -491,9 +491,16 @@ __global__ void __launch_bounds__(kSortThreads, SortTilesPerSm<Loader>::value) r
 // so (the length tag of the ranking keys, the top byte of a skewed alphabet) costs almost no atomics,
 // and a random one one uncontended atomic per key. Warp-uniform trip counts are not needed (no
 // warp-synchronous instruction).
+// Keys read from an array (radixHistogramFrom's source).
 template <class Key>
-__global__ void __launch_bounds__(256) radixHistogram(const Key* __restrict__ keys, uint32_t count, int beginBit,
-                                                      int passes, uint32_t* __restrict__ hist) {
+struct KeyArray {
+    const Key* __restrict__ keys;
+    __device__ __forceinline__ Key operator()(uint64_t i) const { return keys[i]; }
+};
+
+template <class Source>
+__global__ void __launch_bounds__(256) radixHistogramFrom(Source source, uint32_t count, int beginBit, int passes,
+                                                          uint32_t* __restrict__ hist) {
     __shared__ uint32_t h[8][256];
     for (int i = threadIdx.x; i < 8 * 256; i += blockDim.x) (&h[0][0])[i] = 0;
     __syncthreads();
@@ -505,7 +512,7 @@ __global__ void __launch_bounds__(256) radixHistogram(const Key* __restrict__ ke
     }
     const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
     for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < count; i += stride) {
-        const Key k = keys[i];
+        const auto k = source(i);
 #pragma unroll
         for (int p = 0; p < 8; p++) {
             if (p < passes) {
@@ -641,8 +648,8 @@ cudaError_t radixSortPairs(Key*& keys, Key*& keysAlt, uint32_t*& vals, uint32_t*
     const int passes = (endBit - beginBit + 7) / 8;
     SADCS_TRY(cudaMemsetAsync(scratch.digitBase, 0, static_cast<size_t>(passes) * 256 * 4, stream));
     const uint32_t histBlocks = std::min<uint32_t>(ceilDiv(count, 256 * 16), 148 * 8);
-    SADCS_TRY(launch(radixHistogram<Key>, histBlocks, 256, 0, stream, keys, count, beginBit, passes,
-                     scratch.digitBase));
+    SADCS_TRY(launch(radixHistogramFrom<KeyArray<Key>>, histBlocks, 256, 0, stream, KeyArray<Key>{keys}, count,
+                     beginBit, passes, scratch.digitBase));
     SADCS_TRY(launch(radixDigitBase, passes, 256, 0, stream, scratch.digitBase));
     for (int p = 0; p < passes; p++) {
         SortLoader<Key> ld{keys, vals, beginBit + 8 * p};

@@ -67,9 +67,54 @@ __device__ __forceinline__ uint64_t charKey(const TextSet& texts, uint32_t end, 
     return (v << texts.tagBits) | tag;
 }
 
-__global__ void rankInitList(uint32_t* __restrict__ lst, uint32_t m) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < m) lst[i] = i;
+// The first sort of one text: sample i's key is its first characters (charKey at its own
+// position) and its value is i, both made where they are needed: by the digit histograms and by the
+// first radix pass's loader. No key or value array is written or read before that pass.
+struct FirstKeys {
+    TextSet texts;
+    __device__ __forceinline__ uint64_t operator()(uint64_t i) const {
+        return charKey(texts, texts.oneEnd, samplePosition(static_cast<uint32_t>(i)));
+    }
+};
+
+struct FirstKeyLoader {
+    FirstKeys keys;
+    __device__ __forceinline__ bool load(uint32_t, uint32_t i, uint32_t, uint64_t& k, uint32_t& d) const {
+        k = keys(i);
+        d = static_cast<uint32_t>(k) & 0xFF;
+        return true;
+    }
+    __device__ __forceinline__ uint32_t value(uint32_t, uint32_t i, uint32_t) const { return i; }
+};
+
+// Stable LSD sort of samples [0, count) of one text by their first keyChars characters (the
+// ranking's first pass): as radixSortPairs, with the first pass's keys and values made by
+// FirstKeyLoader. On return keys/vals point at the sorted keys and sample indices.
+inline cudaError_t rankFirstSort(const TextSet& texts, uint32_t count, int keyBits, uint64_t*& keys,
+                                 uint64_t*& keysAlt, uint32_t*& vals, uint32_t*& valsAlt, uint32_t* scratchWords,
+                                 cudaStream_t stream) {
+    if (count == 0) return cudaSuccess;
+    const RadixScratch scratch(scratchWords, count);
+    const int passes = (keyBits + 7) / 8;
+    SADCS_TRY(cudaMemsetAsync(scratch.digitBase, 0, static_cast<size_t>(passes) * 256 * 4, stream));
+    const uint32_t histBlocks = std::min<uint32_t>(ceilDiv(count, 256 * 16), 148 * 8);
+    SADCS_TRY(launch(radixHistogramFrom<FirstKeys>, histBlocks, 256, 0, stream, FirstKeys{texts}, count, 0, passes,
+                     scratch.digitBase));
+    SADCS_TRY(launch(radixDigitBase, passes, 256, 0, stream, scratch.digitBase));
+    for (int p = 0; p < passes; p++) {
+        const SortStorer<uint64_t> st{keysAlt, valsAlt, count};
+        if (p == 0) {
+            SADCS_TRY((radixOnesweepPass<uint64_t>(FirstKeyLoader{FirstKeys{texts}}, st, OneSegment{count}, count,
+                                                   ceilDiv(count, kSortTile), scratch.digitBase, scratch, stream)));
+        } else {
+            const SortLoader<uint64_t> ld{keys, vals, 8 * p};
+            SADCS_TRY((radixOnesweepPass<uint64_t>(ld, st, OneSegment{count}, count, ceilDiv(count, kSortTile),
+                                                   scratch.digitBase + p * 256, scratch, stream)));
+        }
+        std::swap(keys, keysAlt);
+        std::swap(vals, valsAlt);
+    }
+    return cudaSuccess;
 }
 
 // doubling == 0: character key at depth; otherwise 1 + rank at p + h. Keys stop at the end of
@@ -406,16 +451,17 @@ inline int bitWidth(uint64_t x) {
 
 // Characters of the first character pass of one text, a global sort of every sample: the fewest
 // whole 8-bit radix passes whose key, tag included, holds enough characters for 2^(chars * bits)
-// to exceed 64 times the samples (on a text without repeats, about 1 sample in 64 then shares its
+// to exceed 16 times the samples (on a text without repeats, about 1 sample in 16 then shares its
 // key with another; a repetitive text leaves its repeats to the later, segmented passes whatever
 // the width), and as many characters as those passes hold, at most keyChars. A narrower key is
 // taken only if it keeps at least kMinFirstPassChars characters: on the 3 GiB genome-like text
-// (2-bit codes) 21 characters in 6 passes took the ranking from 129.6 to 118.1 ms, while on the
-// 256 MiB natural-language-like text (6-bit codes) 6 characters in 5 passes left more suffixes in
-// word-sized repeats for the later passes (17.5 to 19.2 ms).
+// (2-bit codes) 21 characters in 6 passes took the ranking from 129.6 to 118.1 ms, and 17 in 5 (a
+// margin of 16 rather than 64 times the samples) to 89.2 ms against 91.9 with the other changes
+// since, while on the 256 MiB natural-language-like text (6-bit codes) 6 characters in 5 passes
+// left more suffixes in word-sized repeats for the later passes (17.5 to 19.2 ms).
 constexpr uint32_t kMinFirstPassChars = 16;
 #ifndef SADCS_FIRST_PASS_MARGIN_BITS
-#define SADCS_FIRST_PASS_MARGIN_BITS 6  // 2^(chars * bits) >= 2^6 x samples (tuning)
+#define SADCS_FIRST_PASS_MARGIN_BITS 4  // 2^(chars * bits) >= 2^4 x samples (tuning)
 #endif
 inline uint32_t firstPassChars(const TextSet& texts, uint64_t samples) {
     auto width = [](uint32_t x) {
@@ -451,9 +497,7 @@ inline cudaError_t rankSample(const uint8_t* text, const TextSet& texts, uint32_
     if (live == 0) return cudaSuccess;
     uint32_t* cur = b.lst[0];
     uint32_t* alt = b.lst[1];
-    if (texts.count <= 1) {
-        SADCS_TRY(launch(rankInitList, blocks256(live), 256, 0, stream, cur, live));
-    } else {
+    if (texts.count > 1) {  // one text: the first sort makes the list itself (rankFirstSort)
         SADCS_TRY(launch(rankInitTexts, blocks256(slots), 256, 0, stream, texts, sampleBase, slots, cur, ranks));
     }
     uint32_t* error = radixErrorWord(b.scratch);
@@ -478,13 +522,15 @@ inline cudaError_t rankSample(const uint8_t* text, const TextSet& texts, uint32_
         uint64_t* key = b.key[0];
         uint64_t* keyAlt = b.key[1];
         const TextSet& passTexts = first ? firstTexts : texts;
-        SADCS_TRY(launch(rankMakeKeys, blocks256(u), 256, 0, stream, text, ranks, passTexts, lst, key, u, offset,
-                         doubling ? 1 : 0));
+        if (!first) {
+            SADCS_TRY(launch(rankMakeKeys, blocks256(u), 256, 0, stream, text, ranks, passTexts, lst, key, u, offset,
+                             doubling ? 1 : 0));
+        }
         const int keyBits = doubling ? rankBits
                                      : static_cast<int>(passTexts.keyChars * passTexts.bits + passTexts.tagBits);
         if (first) {
-            // Everything in one group: one global sort by subkey.
-            SADCS_TRY(radixSortPairs<uint64_t>(key, keyAlt, lst, lstAlt, u, 0, keyBits, b.scratch, stream));
+            // Everything in one group: one global sort by subkey, its keys made as it goes.
+            SADCS_TRY(rankFirstSort(passTexts, u, keyBits, key, keyAlt, lst, lstAlt, b.scratch, stream));
             SADCS_TRY(cudaMemsetAsync(b.grp, 0, static_cast<size_t>(u) * 4, stream));
         } else {
             // The list holds whole groups in id order: sort inside each group only. Group ids come

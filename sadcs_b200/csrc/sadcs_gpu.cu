@@ -451,7 +451,8 @@ cudaError_t prepareAlphabet(const uint8_t* text, uint64_t total, uint64_t span, 
     SADCS_TRY(cudaMemcpyAsync(decode, decodeHost, 256, cudaMemcpyHostToDevice, stream));
     const KeyShape shape = keyShape(std::max(sigma, 1u));
     const uint64_t words = packedWords(span, shape.bits);
-    SADCS_TRY(launch(packCodes, ceilDiv(words, 256), 256, 0, stream, text, static_cast<uint32_t>(total), table,
+    const uint64_t groups = ceilDiv(words, packGroupChars(shape.bits) * shape.bits / 64);
+    SADCS_TRY(launch(packCodes, ceilDiv(groups, 256), 256, 0, stream, text, static_cast<uint32_t>(total), table,
                      shape.bits, words, packed));
     SADCS_TRY(cudaStreamSynchronize(stream));  // the decode table's host words are reused by the caller
     texts.packed = packed;
