@@ -100,6 +100,15 @@ inline uint32_t* classErrorWord(uint32_t* scratch, uint32_t texts) {
     return radixErrorWord(classRadixScratch(scratch, texts));
 }
 
+// The carried word of position x (one text): 64 bits of the code stream from character x - 1 (code 0
+// before position 0), so the character before x and at least the first 31 characters from x for
+// codes of at most 2 bits. The class passes hand it on (carried(x - 1) is the code of T[x - 2] on
+// top of carried(x) shifted down by one character), so that the final merge reads it in list order
+// instead of gathering it from the text.
+__device__ __forceinline__ uint64_t carriedWord(const uint64_t* __restrict__ packed, uint32_t x, uint32_t bits) {
+    return x ? streamBits(packed, static_cast<uint64_t>(x - 1) * bits) : streamBits(packed, 0) >> bits;
+}
+
 // Class 0: the live sample positions in rank order, list[rank] = position. The ranks of the live
 // samples are a permutation of [0, live), so the slice of ranks [k << shift, (k + 1) << shift)
 // holds exactly 2^shift samples (the last slice the rest). Two steps, so that no write lands at a
@@ -117,34 +126,52 @@ inline uint32_t sampleSliceShift(uint64_t live) {
     return shift;
 }
 
-// fill[k] (zeroed by the caller) counts the pairs placed in slice k so far.
+// fill[k] (zeroed by the caller) counts the pairs placed in slice k so far. kCarry: words[x] = the
+// carried word of the sample in pairs[x] (the samples are read in text order, so are their words).
+template <bool kCarry>
 __global__ void __launch_bounds__(kSliceThreads) classPartitionSample(const uint32_t* __restrict__ ranks,
                                                                      uint32_t slots, uint32_t live, uint32_t shift,
                                                                      TextSet texts, uint32_t* __restrict__ fill,
-                                                                     uint64_t* __restrict__ pairs) {
+                                                                     uint64_t* __restrict__ pairs,
+                                                                     uint64_t* __restrict__ words) {
     __shared__ SliceStage stage;
-    uint64_t v[kSliceItems];
+    uint64_t v[kSliceItems], w[kSliceItems];
     const uint64_t first = static_cast<uint64_t>(blockIdx.x) * kSliceTile + threadIdx.x;
 #pragma unroll
     for (int j = 0; j < kSliceItems; j++) {
         const uint64_t t = first + static_cast<uint64_t>(j) * kSliceThreads;
         v[j] = kNoPair;
+        w[j] = 0;
         if (t < slots) {
             const uint32_t rank = __ldcs(ranks + t);  // streamed: read once
             const uint32_t q = samplePosition(static_cast<uint32_t>(t));
             // a live sample (not past the end or between texts)
-            if (q < texts.endOf(q) && rank < live) v[j] = (static_cast<uint64_t>(rank) << 32) | q;
+            if (q < texts.endOf(q) && rank < live) {
+                v[j] = (static_cast<uint64_t>(rank) << 32) | q;
+                if constexpr (kCarry) w[j] = carriedWord(texts.packed, q, texts.bits);
+            }
         }
     }
-    writeSliceMajor(stage, v, shift, fill, pairs, live);
+    if constexpr (kCarry) {
+        __shared__ SliceCompanion companion;
+        writeSliceMajor(stage, v, shift, fill, pairs, live, &companion, &w, words);
+    } else {
+        writeSliceMajor(stage, v, shift, fill, pairs, live);
+    }
 }
 
-__global__ void classScatterPairs(const uint64_t* __restrict__ pairs, uint32_t live, uint32_t* __restrict__ list) {
+// list[rank] = position of every pair; with carried (one text), also carried[rank] = words[i], the
+// pair's carried word.
+__global__ void classScatterPairs(const uint64_t* __restrict__ pairs, uint32_t live, uint32_t* __restrict__ list,
+                                  uint64_t* __restrict__ carried, const uint64_t* __restrict__ words) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= live) return;
     const uint64_t v = __ldcs(pairs + i);
     const uint32_t r = static_cast<uint32_t>(v >> 32);
-    if (r < live) list[r] = static_cast<uint32_t>(v);
+    if (r < live) {
+        list[r] = static_cast<uint32_t>(v);
+        if (carried) carried[r] = __ldcs(words + i);
+    }
 }
 
 // The class passes consume one character of an element's chain each: pass d keys class d - 1's
@@ -152,17 +179,20 @@ __global__ void classScatterPairs(const uint64_t* __restrict__ pairs, uint32_t l
 // chain holds the codes of the kChainChars characters before p, b bits each: bits [i*b, (i+1)*b)
 // hold the code of T[p - 1 - i] (0 before position 0). The chain travels as the sort key in the
 // narrowest word that holds 6b bits: 16 bits for 2-bit codes (DNA), 32 for up to 5, 64 otherwise.
+// Passes that carry words (one text, codes of at most 2 bits) keep one character more, T[p - 2] of
+// the last pass's elements, the character before that pass's outputs.
 constexpr int kChainChars = kClasses - 1;
+constexpr int kCarryChainChars = kClasses;
 
-template <class Chain>
+template <class Chain, int kChars = kChainChars>
 __device__ __forceinline__ Chain codesBefore(const TextSet& texts, uint32_t p) {
     const uint32_t b = texts.bits;
-    const uint32_t first = p >= kChainChars ? p - kChainChars : 0;
+    const uint32_t first = p >= kChars ? p - kChars : 0;
     const uint64_t window = streamBits(texts.packed, static_cast<uint64_t>(first) * b);  // >= 8 codes
     const uint64_t mask = (uint64_t(1) << b) - 1;
     uint64_t chain = 0;
 #pragma unroll
-    for (int i = 0; i < kChainChars; i++) {
+    for (int i = 0; i < kChars; i++) {
         const int at = static_cast<int>(p - first) - 1 - i;  // T[p - 1 - i] is character `at` of the window
         if (at >= 0) chain |= ((window >> (64 - (at + 1) * b)) & mask) << (b * i);
     }
@@ -178,15 +208,18 @@ __device__ __forceinline__ Chain codesBefore(const TextSet& texts, uint32_t p) {
 #define SADCS_CLASS_TILES 4  // onesweep tiles per SM of the class passes (tuning)
 #endif
 
-template <class Chain>
+template <class Chain, bool kCarryWords = false>
 struct ClassLoader {
     // 4 tiles per SM (64 registers, some spilled) against 3 (80 registers): the class phase of the
     // 3 GiB genome-like text took 64.0 ms against 67.9, of the 256 MiB natural text 4.86 against 5.11
     // (64-bit chains).
     static constexpr int kTilesPerSm = SADCS_CLASS_TILES;
+    static constexpr bool kCarry = kCarryWords;
+    static constexpr int kChars = kCarryWords ? kCarryChainChars : kChainChars;
     const uint32_t* __restrict__ lists;       // global lists
     const uint32_t* __restrict__ prevOffset;  // rowBase row of class d - 1: text j's slice offset
     const Chain* __restrict__ chains;         // chains of class d - 1 by index from prevStart (d >= 2)
+    const uint64_t* __restrict__ carried;     // kCarryWords: carried words by global slot
     uint32_t prevStart;                       // first slot of class d - 1 in the global lists
     TextSet texts;
     uint32_t d;
@@ -201,11 +234,21 @@ struct ClassLoader {
         const bool stored = k > 0 && d > 1;
         const Chain chain = stored ? chains[__ldg(prevOffset + j) - prevStart + k - 1] : Chain(0);
         if (p <= start || p > end || classOfResidue((p - 1) % kV) != d) return false;
-        key = stored ? chain : codesBefore<Chain>(texts, p);
+        key = stored ? chain : codesBefore<Chain, kChars>(texts, p);
         dig = static_cast<uint32_t>(key) & ((1u << texts.bits) - 1);  // codes order like the bytes they stand for
         return true;
     }
     __device__ __forceinline__ uint32_t value(uint32_t j, uint32_t, uint32_t k) const { return element(j, k) - 1; }
+    // The code of T[p - 2], the character before the output p - 1.
+    __device__ __forceinline__ uint8_t carryTag(Chain key) const {
+        return static_cast<uint8_t>((static_cast<uint32_t>(key) >> texts.bits) & ((1u << texts.bits) - 1));
+    }
+    // carried(p - 1) from carried(p) (the text's end: from the code stream).
+    __device__ __forceinline__ uint64_t carry(uint32_t j, uint32_t, uint32_t k, uint32_t tag) const {
+        if (k == 0) return carriedWord(texts.packed, texts.endOfText(j) - 1, texts.bits);
+        const uint64_t from = carried[__ldg(prevOffset + j) + k - 1];
+        return (static_cast<uint64_t>(tag) << (64 - texts.bits)) | (from >> texts.bits);
+    }
 };
 
 // Writes class d's positions, and (unless chains is null: the last class) the chains of its
@@ -215,6 +258,7 @@ struct ClassStorer {
     static constexpr bool kKeys = true;
     uint32_t* __restrict__ lists;
     Chain* __restrict__ chains;  // by index from lo
+    uint64_t* __restrict__ carried;  // carried words by global slot (loaders that carry them)
     uint32_t lo, hi;             // class d's slots in the global lists
     uint32_t bits;
     __device__ __forceinline__ void storeKey(uint32_t, uint32_t pos, Chain chain) const {
@@ -222,6 +266,9 @@ struct ClassStorer {
     }
     __device__ __forceinline__ void storeValue(uint32_t, uint32_t pos, uint32_t v) const {
         if (pos >= lo && pos < hi) lists[pos] = v;  // always, unless a look-back timed out
+    }
+    __device__ __forceinline__ void storeCarry(uint32_t, uint32_t pos, uint64_t w) const {
+        if (pos >= lo && pos < hi) carried[pos] = w;
     }
 };
 
@@ -272,34 +319,41 @@ __global__ void __launch_bounds__(256) classDigitBase(uint32_t* __restrict__ his
     row[threadIdx.x] = rowBase[blockIdx.x] + inclusive - v;
 }
 
-// Passes 1 to kClasses - 1: class d from class d - 1, chains of type Chain in the two chain buffers.
-template <class Chain>
+// Passes 1 to kClasses - 1: class d from class d - 1, chains of type Chain in the two chain buffers;
+// kCarry: the carried words too (carried: by global slot).
+template <class Chain, bool kCarry = false>
 inline cudaError_t classPasses(const TextSet& texts, const ClassPlan& plan, const ClassTables& tables, uint32_t* lists,
                                const uint32_t* hist, const RadixScratch& radix, uint64_t* const chains[2],
-                               cudaStream_t stream) {
+                               uint64_t* carried, cudaStream_t stream) {
     const uint32_t J = tables.texts;
     for (int d = 1; d < kClasses; d++) {
         if (plan.start[d + 1] == plan.start[d]) continue;
-        ClassLoader<Chain> ld{lists, tables.rowBase + static_cast<size_t>(d - 1) * J,
-                              reinterpret_cast<const Chain*>(chains[d & 1]), plan.start[d - 1], texts,
-                              static_cast<uint32_t>(d)};
+        ClassLoader<Chain, kCarry> ld{lists, tables.rowBase + static_cast<size_t>(d - 1) * J,
+                                      reinterpret_cast<const Chain*>(chains[d & 1]), carried, plan.start[d - 1],
+                                      texts, static_cast<uint32_t>(d)};
         ClassStorer<Chain> st{lists, d + 1 < kClasses ? reinterpret_cast<Chain*>(chains[(d + 1) & 1]) : nullptr,
-                              plan.start[d], plan.start[d + 1], texts.bits};
+                              carried, plan.start[d], plan.start[d + 1], texts.bits};
         ManySegments segs{tables.tileStart + static_cast<size_t>(d) * (J + 1),
                           tables.elementStart + static_cast<size_t>(d) * (J + 1), J};
-        SADCS_TRY((radixOnesweepPass<Chain, ClassLoader<Chain>, ClassStorer<Chain>, ManySegments>(
+        SADCS_TRY((radixOnesweepPass<Chain, ClassLoader<Chain, kCarry>, ClassStorer<Chain>, ManySegments>(
             ld, st, segs, plan.inputs[d], plan.tiles[d], hist + static_cast<size_t>(d) * J * 256, radix, stream)));
     }
     return cudaSuccess;
 }
 
+// Whether a construction carries words through the class passes: one text with codes of at most 2
+// bits (the final merge's records are then one word).
+inline bool carriesWords(const TextSet& texts) { return texts.count == 1 && texts.bits <= 2; }
+
 // Fills lists (laid out by plan.start, text-major inside each class) from the sample ranks.
 // tables: the ClassTables block on the device; scratch: classScratchWords(total, J) words.
 // total: bytes of the concatenation (text buffer) scanned by the histogram.
-// chains: two buffers of classChainWords(plan) 64-bit words each.
+// chains: two buffers of classChainWords(plan) 64-bit words each. carried: null, or (carriesWords)
+// one word per list slot, filled with every element's carried word.
 inline cudaError_t sortClasses(uint32_t total, const TextSet& texts, const uint32_t* ranks, uint32_t slots,
                                const ClassPlan& plan, const ClassTables& tables, uint32_t* lists, uint32_t* scratch,
-                               uint64_t* const chains[2], cudaStream_t stream) {
+                               uint64_t* const chains[2], uint64_t* carried, cudaStream_t stream) {
+    if (carried && !carriesWords(texts)) return cudaErrorInvalidValue;
     const uint32_t J = tables.texts;
     const uint32_t live = plan.start[1];
     uint32_t* hist = scratch;  // [kClasses][J][256]
@@ -308,21 +362,30 @@ inline cudaError_t sortClasses(uint32_t total, const TextSet& texts, const uint3
     // (the radix scratch's digit-base words, unused by the class passes).
     uint32_t* fill = radix.digitBase;
     SADCS_TRY(cudaMemsetAsync(fill, 0, kMaxSampleSlices * sizeof(uint32_t), stream));
-    SADCS_TRY(launch(classPartitionSample, ceilDiv(slots, kSliceTile), kSliceThreads, 0, stream, ranks, slots, live,
-                     sampleSliceShift(live), texts, fill, chains[0]));
-    SADCS_TRY(launch(classScatterPairs, ceilDiv(live, 256), 256, 0, stream, chains[0], live, lists));
+    // (with carried words: the pairs' words in chain buffer 1, also free until pass 1)
+    if (carried) {
+        SADCS_TRY(launch(classPartitionSample<true>, ceilDiv(slots, kSliceTile), kSliceThreads, 0, stream, ranks, slots,
+                         live, sampleSliceShift(live), texts, fill, chains[0], chains[1]));
+    } else {
+        SADCS_TRY(launch(classPartitionSample<false>, ceilDiv(slots, kSliceTile), kSliceThreads, 0, stream, ranks,
+                         slots, live, sampleSliceShift(live), texts, fill, chains[0], nullptr));
+    }
+    SADCS_TRY(launch(classScatterPairs, ceilDiv(live, 256), 256, 0, stream, chains[0], live, lists, carried,
+                     chains[1]));
     SADCS_TRY(cudaMemsetAsync(hist, 0, static_cast<size_t>(kClasses) * J * 256 * 4, stream));
     SADCS_TRY(cudaMemsetAsync(radix.control, 0, 8, stream));
     const uint32_t blocks = std::min<uint32_t>(ceilDiv(total + 7ull, 256 * 8 * 8), 148 * 8);
     SADCS_TRY(launch(classHistogram, std::max(blocks, 1u), 256, 0, stream, total, texts, hist));
     SADCS_TRY(launch(classDigitBase, kClasses * J, 256, 0, stream, hist, tables.rowBase));
+    static_assert(2 * kCarryChainChars <= 16, "carrying chains of 2-bit codes fit 16 bits");
+    if (carried) return classPasses<uint16_t, true>(texts, plan, tables, lists, hist, radix, chains, carried, stream);
     if (texts.bits * kChainChars <= 16) {
-        return classPasses<uint16_t>(texts, plan, tables, lists, hist, radix, chains, stream);
+        return classPasses<uint16_t>(texts, plan, tables, lists, hist, radix, chains, nullptr, stream);
     }
     if (texts.bits * kChainChars <= 32) {
-        return classPasses<uint32_t>(texts, plan, tables, lists, hist, radix, chains, stream);
+        return classPasses<uint32_t>(texts, plan, tables, lists, hist, radix, chains, nullptr, stream);
     }
-    return classPasses<uint64_t>(texts, plan, tables, lists, hist, radix, chains, stream);
+    return classPasses<uint64_t>(texts, plan, tables, lists, hist, radix, chains, nullptr, stream);
 }
 
 }  // namespace sadcs

@@ -96,6 +96,7 @@ struct MergeArgs {
     uint32_t* const* saTexts;  // level 0, optional, in place of sa: one output array per text
     uint8_t* const* bwtTexts;  // level 0, optional, in place of bwt: one output array per text
     uint32_t* error;         // set nonzero if a window set exceeds the capacity (never, by construction)
+    const uint64_t* carried;  // level 0, optional: every list slot's carried word (one text, 1-word records)
 };
 
 // The top `bits` bits set (bits <= 64).
@@ -364,7 +365,8 @@ inline cudaError_t mergeClasses(const uint8_t* text, const uint32_t* ranks, cons
                                 uint32_t* rowZero, uint32_t* splitters, MergeRow* rows, uint32_t* sa, uint8_t* bwt,
                                 uint32_t* counter, uint32_t* hostWord, cudaStream_t stream,
                                 cudaEvent_t finalStart = nullptr, cudaEvent_t finalStop = nullptr,
-                                uint32_t* const* saTexts = nullptr, uint8_t* const* bwtTexts = nullptr) {
+                                uint32_t* const* saTexts = nullptr, uint8_t* const* bwtTexts = nullptr,
+                                const uint64_t* carried = nullptr) {
     MergeLevel level[kMaxLevels];
     for (int L = 0; L <= plan.top; L++) {
         level[L].lists = L == 0 ? lists : splitters + plan.listWord[L];
@@ -400,6 +402,7 @@ inline cudaError_t mergeClasses(const uint8_t* text, const uint32_t* ranks, cons
         if (L == 0) {
             args.sa = sa;
             args.bwt = bwt;
+            args.carried = carried;
             if (finalStart) SADCS_TRY(cudaEventRecord(finalStart, stream));
             SADCS_TRY(launchTree<true>(args, tiles, stream));
             if (finalStop) SADCS_TRY(cudaEventRecord(finalStop, stream));

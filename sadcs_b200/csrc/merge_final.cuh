@@ -204,120 +204,13 @@ constexpr int mergeTilesPerSm() {
     return W == 1 ? SADCS_MERGE_TILES_W1 : 4;
 }
 
-// kFinal: the last level, writing the SA and the BWT; otherwise an upper level, writing the rows
-// (every R-th element of the merged order with its per-list counts) that bound the tiles below.
+// The merge tree over a gathered tile, and its outputs: the SA and BWT (kFinal) or the rows.
 template <int W, bool kMulti, bool kFinal>
-__global__ void __launch_bounds__(mergeThreads(W), mergeTilesPerSm<W>()) mergeTree(MergeArgs a) {
+__device__ __forceinline__ void mergeTileTail(const MergeArgs& a, const FinalTile<W, kMulti>& s, const MergeTileInfo& t,
+                                              const uint32_t* bounds, uint32_t size, uint32_t n, uint32_t bits,
+                                              uint32_t& sLo, uint32_t& sHi) {
     constexpr int kMergeThreads = mergeThreads(W);
     constexpr uint32_t kMergeR = mergeR(W);
-    constexpr uint32_t kMergeCap = FinalTile<W, kMulti>::kMergeCap;
-    extern __shared__ __align__(16) unsigned char smem[];
-    FinalTile<W, kMulti> s;
-    s.carve(smem, a.ranks);
-    __shared__ MergeTileInfo t;
-    __shared__ uint32_t sLo, sHi;
-    __shared__ uint32_t bounds[3 * 7];  // the tree's merges: 4 + 2 + 1 triples of window offsets
-    if (threadIdx.x < 32) {
-        planTileWindows(a, kMergeCap, t);
-        __syncwarp();
-        // (0,1) (2,3) (4,5) (6,-), then (01,23) (45,6), then (0123,456): indices into t.seg, 3 bits
-        // each (a register constant: a table indexed by the lane would live in local memory)
-        constexpr uint8_t kTree[21] = {0, 1, 2, 2, 3, 4, 4, 5, 6, 6, 7, 7, 0, 2, 4, 4, 6, 7, 0, 4, 7};
-        constexpr uint64_t kTreePacked = [] {
-            uint64_t v = 0;
-            for (int i = 0; i < 21; i++) v |= static_cast<uint64_t>(kTree[i]) << (3 * i);
-            return v;
-        }();
-        if (threadIdx.x < 21) bounds[threadIdx.x] = t.seg[(kTreePacked >> (3 * threadIdx.x)) & 7];
-        if (threadIdx.x == 0) {
-            sLo = 0;
-            sHi = t.size;
-            if (t.bad && a.error) atomicExch(a.error, 1u);
-        }
-    }
-    __syncthreads();
-    if (t.bad) return;
-    const uint32_t size = t.size;
-    const uint32_t* st = a.level.start;
-    const uint32_t bits = a.texts.bits;
-    const uint32_t n = kMulti ? 0u : a.texts.oneEnd;
-
-    // Gather: positions from the lists (coalesced), then each record's code words and ranks by
-    // asynchronous copies, all in flight at once; the word after them and the word before them
-    // (when the previous character starts there) by plain loads, also in flight.
-    constexpr int kItems = (kMergeCap + kMergeThreads - 1) / kMergeThreads;
-    uint32_t p[kItems];
-    uint64_t extra[kItems], before[kItems];
-    // Positions first, every list load in flight at once (an asynchronous copy between two loads
-    // would order them), then the records' copies.
-#pragma unroll
-    for (int j = 0; j < kItems; j++) {
-        const uint32_t e = threadIdx.x + j * kMergeThreads;
-        p[j] = 0;
-        if (e < size) {
-            const int l = listOfElement(t.seg, e);
-            p[j] = a.level.lists[st[l] + t.win[l] + (e - t.seg[l])];
-        }
-    }
-    // The end of each position's text (several texts: one load chain per item, all in flight).
-    uint32_t ends[kMulti ? kItems : 1];
-    if constexpr (kMulti) {
-#pragma unroll
-        for (int j = 0; j < kItems; j++) ends[j] = threadIdx.x + j * kMergeThreads < size ? a.texts.endOf(p[j]) : 0;
-    }
-#pragma unroll
-    for (int j = 0; j < kItems; j++) {
-        const uint32_t e = threadIdx.x + j * kMergeThreads;
-        if (e < size) {
-            uint32_t q = p[j];
-            const uint32_t qEnd = kMulti ? ends[j] : a.texts.oneEnd;
-            if (q >= qEnd) {  // cannot happen for valid class lists; never read out of range
-                atomicExch(a.error, 3u);
-                q = 0;
-            }
-            p[j] = q;
-            s.pos[e] = q;
-            if constexpr (kMulti) s.end[e] = q < qEnd ? qEnd : a.texts.endOf(0);
-            const uint64_t* src = a.texts.packed + ((static_cast<uint64_t>(q) * bits) >> 6);
-#pragma unroll
-            for (int w = 0; w < W; w++) cpAsync8(&s.words[w * kMergeCap + e], src + w);
-        }
-    }
-#pragma unroll
-    for (int j = 0; j < kItems; j++) {
-        const uint32_t e = threadIdx.x + j * kMergeThreads;
-        extra[j] = 0;
-        before[j] = 0;
-        if (e < size) {
-            const uint64_t bit = static_cast<uint64_t>(p[j]) * bits;
-            const uint64_t w0 = bit >> 6;
-            extra[j] = __ldg(a.texts.packed + w0 + W);
-            if (kFinal && (bit & 63) < bits && w0 > 0) before[j] = __ldg(a.texts.packed + w0 - 1);
-        }
-    }
-    cpAsyncWaitAll();
-#pragma unroll
-    for (int j = 0; j < kItems; j++) {
-        const uint32_t e = threadIdx.x + j * kMergeThreads;
-        if (e < size) {
-            const uint32_t o = static_cast<uint32_t>((static_cast<uint64_t>(p[j]) * bits) & 63);
-            uint64_t r[W + 1];
-#pragma unroll
-            for (int w = 0; w < W; w++) r[w] = s.words[w * kMergeCap + e];
-            r[W] = extra[j];
-            // the character before p ends at bit o of word 0: bits [64 + o - b, 64 + o) of before:r[0]
-            if constexpr (kFinal) {
-                const uint64_t window = o ? (before[j] << o) | (r[0] >> (64 - o)) : before[j];
-                s.prev[e] = static_cast<uint8_t>(window & ((1u << bits) - 1));
-            }
-            if (o) {
-#pragma unroll
-                for (int w = 0; w < W; w++) s.words[w * kMergeCap + e] = (r[w] << o) | (r[w + 1] >> (64 - o));
-            }
-        }
-    }
-    __syncthreads();
-
     // The merge tree.
     finalLevel<W, kMulti, true>(s, nullptr, s.idxB, bounds, 4, size, n, bits);
     __syncthreads();
@@ -397,6 +290,165 @@ __global__ void __launch_bounds__(mergeThreads(W), mergeTilesPerSm<W>()) mergeTr
             a.rowsOut[g / kMergeR] = row;
         }
     }
+}
+
+// kFinal: the last level, writing the SA and the BWT; otherwise an upper level, writing the rows
+// (every R-th element of the merged order with its per-list counts) that bound the tiles below.
+template <int W, bool kMulti, bool kFinal>
+__global__ void __launch_bounds__(mergeThreads(W), mergeTilesPerSm<W>()) mergeTree(MergeArgs a) {
+    constexpr int kMergeThreads = mergeThreads(W);
+    constexpr uint32_t kMergeR = mergeR(W);
+    constexpr uint32_t kMergeCap = FinalTile<W, kMulti>::kMergeCap;
+    extern __shared__ __align__(16) unsigned char smem[];
+    FinalTile<W, kMulti> s;
+    s.carve(smem, a.ranks);
+    __shared__ MergeTileInfo t;
+    __shared__ uint32_t sLo, sHi;
+    __shared__ uint32_t bounds[3 * 7];  // the tree's merges: 4 + 2 + 1 triples of window offsets
+    if (threadIdx.x < 32) {
+        planTileWindows(a, kMergeCap, t);
+        __syncwarp();
+        // (0,1) (2,3) (4,5) (6,-), then (01,23) (45,6), then (0123,456): indices into t.seg, 3 bits
+        // each (a register constant: a table indexed by the lane would live in local memory)
+        constexpr uint8_t kTree[21] = {0, 1, 2, 2, 3, 4, 4, 5, 6, 6, 7, 7, 0, 2, 4, 4, 6, 7, 0, 4, 7};
+        constexpr uint64_t kTreePacked = [] {
+            uint64_t v = 0;
+            for (int i = 0; i < 21; i++) v |= static_cast<uint64_t>(kTree[i]) << (3 * i);
+            return v;
+        }();
+        if (threadIdx.x < 21) bounds[threadIdx.x] = t.seg[(kTreePacked >> (3 * threadIdx.x)) & 7];
+        if (threadIdx.x == 0) {
+            sLo = 0;
+            sHi = t.size;
+            if (t.bad && a.error) atomicExch(a.error, 1u);
+        }
+    }
+    __syncthreads();
+    if (t.bad) return;
+    const uint32_t size = t.size;
+    const uint32_t* st = a.level.start;
+    const uint32_t bits = a.texts.bits;
+    const uint32_t n = kMulti ? 0u : a.texts.oneEnd;
+
+    constexpr int kItems = (kMergeCap + kMergeThreads - 1) / kMergeThreads;
+    if constexpr (kFinal && W == 1 && !kMulti) {
+        if (a.carried) {
+            // Carried words (one text): each record's code word and previous character come with its
+            // position, read in list order beside it (half of a thread's items in flight at a time:
+            // all of them would not fit the register budget).
+            constexpr int kHalf = (kItems + 1) / 2;
+#pragma unroll
+            for (int h = 0; h < kItems; h += kHalf) {
+                uint32_t p[kHalf];
+                uint64_t c[kHalf];
+#pragma unroll
+                for (int j = 0; j < kHalf; j++) {
+                    const uint32_t e = threadIdx.x + (h + j) * kMergeThreads;
+                    p[j] = 0;
+                    c[j] = 0;
+                    if (h + j < kItems && e < size) {
+                        const int l = listOfElement(t.seg, e);
+                        const uint32_t slot = st[l] + t.win[l] + (e - t.seg[l]);
+                        p[j] = a.level.lists[slot];
+                        c[j] = a.carried[slot];
+                    }
+                }
+#pragma unroll
+                for (int j = 0; j < kHalf; j++) {
+                    const uint32_t e = threadIdx.x + (h + j) * kMergeThreads;
+                    if (h + j < kItems && e < size) {
+                        uint32_t q = p[j];
+                        if (q >= n) {  // cannot happen for valid class lists; never read out of range
+                            atomicExch(a.error, 3u);
+                            q = 0;
+                        }
+                        s.pos[e] = q;
+                        s.words[e] = c[j] << bits;
+                        s.prev[e] = static_cast<uint8_t>(c[j] >> (64 - bits));
+                    }
+                }
+            }
+            __syncthreads();
+            mergeTileTail<W, kMulti, kFinal>(a, s, t, bounds, size, n, bits, sLo, sHi);
+            return;
+        }
+    }
+
+    // Gather: positions from the lists (coalesced), then each record's code words and ranks by
+    // asynchronous copies, all in flight at once; the word after them and the word before them
+    // (when the previous character starts there) by plain loads, also in flight.
+    uint32_t p[kItems];
+    uint64_t extra[kItems], before[kItems];
+    // Positions first, every list load in flight at once (an asynchronous copy between two loads
+    // would order them), then the records' copies.
+#pragma unroll
+    for (int j = 0; j < kItems; j++) {
+        const uint32_t e = threadIdx.x + j * kMergeThreads;
+        p[j] = 0;
+        if (e < size) {
+            const int l = listOfElement(t.seg, e);
+            p[j] = a.level.lists[st[l] + t.win[l] + (e - t.seg[l])];
+        }
+    }
+    // The end of each position's text (several texts: one load chain per item, all in flight).
+    uint32_t ends[kMulti ? kItems : 1];
+    if constexpr (kMulti) {
+#pragma unroll
+        for (int j = 0; j < kItems; j++) ends[j] = threadIdx.x + j * kMergeThreads < size ? a.texts.endOf(p[j]) : 0;
+    }
+#pragma unroll
+    for (int j = 0; j < kItems; j++) {
+        const uint32_t e = threadIdx.x + j * kMergeThreads;
+        if (e < size) {
+            uint32_t q = p[j];
+            const uint32_t qEnd = kMulti ? ends[j] : a.texts.oneEnd;
+            if (q >= qEnd) {  // cannot happen for valid class lists; never read out of range
+                atomicExch(a.error, 3u);
+                q = 0;
+            }
+            p[j] = q;
+            s.pos[e] = q;
+            if constexpr (kMulti) s.end[e] = q < qEnd ? qEnd : a.texts.endOf(0);
+            const uint64_t* src = a.texts.packed + ((static_cast<uint64_t>(q) * bits) >> 6);
+#pragma unroll
+            for (int w = 0; w < W; w++) cpAsync8(&s.words[w * kMergeCap + e], src + w);
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < kItems; j++) {
+        const uint32_t e = threadIdx.x + j * kMergeThreads;
+        extra[j] = 0;
+        before[j] = 0;
+        if (e < size) {
+            const uint64_t bit = static_cast<uint64_t>(p[j]) * bits;
+            const uint64_t w0 = bit >> 6;
+            extra[j] = __ldg(a.texts.packed + w0 + W);
+            if (kFinal && (bit & 63) < bits && w0 > 0) before[j] = __ldg(a.texts.packed + w0 - 1);
+        }
+    }
+    cpAsyncWaitAll();
+#pragma unroll
+    for (int j = 0; j < kItems; j++) {
+        const uint32_t e = threadIdx.x + j * kMergeThreads;
+        if (e < size) {
+            const uint32_t o = static_cast<uint32_t>((static_cast<uint64_t>(p[j]) * bits) & 63);
+            uint64_t r[W + 1];
+#pragma unroll
+            for (int w = 0; w < W; w++) r[w] = s.words[w * kMergeCap + e];
+            r[W] = extra[j];
+            // the character before p ends at bit o of word 0: bits [64 + o - b, 64 + o) of before:r[0]
+            if constexpr (kFinal) {
+                const uint64_t window = o ? (before[j] << o) | (r[0] >> (64 - o)) : before[j];
+                s.prev[e] = static_cast<uint8_t>(window & ((1u << bits) - 1));
+            }
+            if (o) {
+#pragma unroll
+                for (int w = 0; w < W; w++) s.words[w * kMergeCap + e] = (r[w] << o) | (r[w + 1] >> (64 - o));
+            }
+        }
+    }
+    __syncthreads();
+    mergeTileTail<W, kMulti, kFinal>(a, s, t, bounds, size, n, bits, sLo, sHi);
 }
 
 // Launches a level (kFinal: the last) for the texts' code width (W words per record) and text count.

@@ -179,12 +179,21 @@ struct SliceStage {
     uint64_t pairs[kSliceTile];
 };
 
+// A companion word per pair (writeSliceMajor's second form) goes to the same place of a second
+// array, staged after the pairs in the same buffer; the slice of every staged slot is kept for it.
+struct SliceCompanion {
+    uint8_t slice[kSliceTile];
+};
+
 // All threads of the block, each with its kSliceItems pairs (kNoPair where it has none, and for
 // any pair whose slice is not below kMaxSlices). fill[k] (zeroed by the caller before the launch)
-// counts the pairs placed in slice k; capacity bounds the pair array.
+// counts the pairs placed in slice k; capacity bounds the pair array. With a companion (cs, w,
+// dstW non-null), w[j] is written to dstW at the place v[j] goes to in dst.
 __device__ __forceinline__ void writeSliceMajor(SliceStage& st, const uint64_t (&v)[kSliceItems], uint32_t shift,
                                                 uint32_t* __restrict__ fill, uint64_t* __restrict__ dst,
-                                                uint64_t capacity) {
+                                                uint64_t capacity, SliceCompanion* cs = nullptr,
+                                                const uint64_t (*w)[kSliceItems] = nullptr,
+                                                uint64_t* __restrict__ dstW = nullptr) {
     for (uint32_t i = threadIdx.x; i < kMaxSlices; i += kSliceThreads) st.count[i] = 0;
     __syncthreads();
     uint32_t local[kSliceItems];
@@ -230,6 +239,21 @@ __device__ __forceinline__ void writeSliceMajor(SliceStage& st, const uint64_t (
         const uint32_t rel = st.base[k] + (i - st.offset[k]);
         const uint64_t at = (static_cast<uint64_t>(k) << shift) + rel;
         if ((static_cast<uint64_t>(rel) >> shift) == 0 && at < capacity) dst[at] = pair;  // always, by construction
+        if (cs) cs->slice[i] = static_cast<uint8_t>(k);
+    }
+    if (cs) {
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < kSliceItems; j++) {
+            if (v[j] != kNoPair) st.pairs[st.offset[static_cast<uint32_t>(v[j] >> 32) >> shift] + local[j]] = (*w)[j];
+        }
+        __syncthreads();
+        for (uint32_t i = threadIdx.x; i < total; i += kSliceThreads) {
+            const uint32_t k = cs->slice[i];
+            const uint32_t rel = st.base[k] + (i - st.offset[k]);
+            const uint64_t at = (static_cast<uint64_t>(k) << shift) + rel;
+            if ((static_cast<uint64_t>(rel) >> shift) == 0 && at < capacity) dstW[at] = st.pairs[i];
+        }
     }
 }
 
@@ -260,9 +284,11 @@ constexpr uint32_t kMaxSortCount = kStatusValue;
 constexpr long long kLookbackLimitCycles = 4000000000ll;
 
 // Shared memory of radixOnesweep for a key of keyBytes bytes: one staging buffer that holds the
-// tile's keys and then its values, the digit of every staged slot, and the counting tables.
-constexpr size_t radixSharedBytes(size_t keyBytes) {
-    return kSortTile * (keyBytes > 4 ? keyBytes : 4) + kSortTile + (kSortWarps * 256 + 256 + 256 + 32) * 4 + 64;
+// tile's keys, then its values, then (carry) its 64-bit carried words; the digit of every staged
+// slot, (carry) a tag byte per slot, and the counting tables.
+constexpr size_t radixSharedBytes(size_t keyBytes, bool carry = false) {
+    const size_t stage = carry ? 8 : (keyBytes > 4 ? keyBytes : 4);
+    return kSortTile * stage + kSortTile * (carry ? 2 : 1) + (kSortWarps * 256 + 256 + 256 + 32) * 4 + 64;
 }
 
 // Segments of a pass: element ranges sorted independently, each from its own digit bases, with
@@ -316,6 +342,18 @@ struct SortTilesPerSm<Loader, std::void_t<decltype(Loader::kTilesPerSm)>> {
     static constexpr int value = Loader::kTilesPerSm;
 };
 
+// A loader may carry a 64-bit word with every element (kCarry): it gives a tag byte from the key
+// (carryTag), staged while the key is in registers, and after the look-back the element's carried
+// word from its index and that tag (carry); the storer writes it (storeCarry).
+template <class Loader, class = void>
+struct LoaderCarries {
+    static constexpr bool value = false;
+};
+template <class Loader>
+struct LoaderCarries<Loader, std::void_t<decltype(Loader::kCarry)>> {
+    static constexpr bool value = Loader::kCarry;
+};
+
 template <class Key, class Loader, class Storer, class Segments = OneSegment>
 __global__ void __launch_bounds__(kSortThreads, SortTilesPerSm<Loader>::value) radixOnesweep(Loader ld, Storer st, Segments segs,
                                                                  const uint32_t* __restrict__ digitBase,
@@ -324,11 +362,14 @@ __global__ void __launch_bounds__(kSortThreads, SortTilesPerSm<Loader>::value) r
                                                                  uint32_t* __restrict__ error,
                                                                  long long lookbackLimit) {
     extern __shared__ __align__(16) unsigned char smem[];
-    constexpr size_t kStageBytes = kSortTile * (sizeof(Key) > 4 ? sizeof(Key) : 4);
+    constexpr bool kCarry = LoaderCarries<Loader>::value;
+    constexpr size_t kStageBytes = kSortTile * (kCarry ? 8 : (sizeof(Key) > 4 ? sizeof(Key) : 4));
     Key* sKeys = reinterpret_cast<Key*>(smem);
     uint32_t* sVals = reinterpret_cast<uint32_t*>(smem);  // the same buffer, after the keys are out
+    uint64_t* sCarry = reinterpret_cast<uint64_t*>(smem);  // and after the values
     uint8_t* sDig = smem + kStageBytes;
-    uint32_t* warpCount = reinterpret_cast<uint32_t*>(sDig + kSortTile);
+    uint8_t* sTag = sDig + kSortTile;  // carry only
+    uint32_t* warpCount = reinterpret_cast<uint32_t*>(sDig + kSortTile * (kCarry ? 2 : 1));
     uint32_t* digitStart = warpCount + kSortWarps * 256;
     uint32_t* digitGlobal = digitStart + 256;
     uint32_t* warpTotals = digitGlobal + 256;
@@ -406,6 +447,7 @@ __global__ void __launch_bounds__(kSortThreads, SortTilesPerSm<Loader>::value) r
             const uint32_t slot = digitStart[dj] + warpCount[warp * 256 + dj] + (rankDigit[j] >> 9);
             if constexpr (Storer::kKeys) sKeys[slot] = keys[j];
             sDig[slot] = static_cast<uint8_t>(dj);
+            if constexpr (kCarry) sTag[slot] = ld.carryTag(keys[j]);
             rankDigit[j] = slot;  // from here on: the item's staged slot
             const uint64_t i = warpBase + j * 32 + lane;
             vals[j] = ld.value(segment, segBegin + static_cast<uint32_t>(i), static_cast<uint32_t>(i));
@@ -482,6 +524,29 @@ __global__ void __launch_bounds__(kSortThreads, SortTilesPerSm<Loader>::value) r
     for (uint32_t i = threadIdx.x; i < tileTotal; i += kSortThreads) {
         const uint32_t dj = sDig[i];
         st.storeValue(segment, digitGlobal[dj] + i - digitStart[dj], sVals[i]);
+    }
+    if constexpr (kCarry) {
+        // The carried words: read in element order (every read in flight), staged by slot, written.
+        uint64_t carried[kSortItems];
+#pragma unroll
+        for (int j = 0; j < kSortItems; j++) {
+            const uint64_t i = warpBase + j * 32 + lane;
+            carried[j] = 0;
+            if (rankDigit[j] != 0xFFFFFFFFu) {
+                carried[j] = ld.carry(segment, segBegin + static_cast<uint32_t>(i), static_cast<uint32_t>(i),
+                                      sTag[rankDigit[j]]);
+            }
+        }
+        __syncthreads();  // the values are out of the staging buffer
+#pragma unroll
+        for (int j = 0; j < kSortItems; j++) {
+            if (rankDigit[j] != 0xFFFFFFFFu) sCarry[rankDigit[j]] = carried[j];
+        }
+        __syncthreads();
+        for (uint32_t i = threadIdx.x; i < tileTotal; i += kSortThreads) {
+            const uint32_t dj = sDig[i];
+            st.storeCarry(segment, digitGlobal[dj] + i - digitStart[dj], sCarry[i]);
+        }
     }
 }
 
@@ -626,7 +691,7 @@ cudaError_t radixOnesweepPass(const Loader& ld, const Storer& st, const Segments
     SADCS_TRY(cudaMemsetAsync(scratch.status, 0, static_cast<size_t>(tiles + skipTiles) * 256 * 4, stream));
     SADCS_TRY(cudaMemsetAsync(scratch.control, 0, 4, stream));
     if (skipTiles) SADCS_TRY(cudaMemsetAsync(scratch.control, static_cast<int>(skipTiles), 1, stream));
-    constexpr size_t shared = radixSharedBytes(sizeof(Key));
+    constexpr size_t shared = radixSharedBytes(sizeof(Key), LoaderCarries<Loader>::value);
     // The opt-in above 48 KiB of dynamic shared memory is per function and per device.
     static std::atomic<uint64_t> configured{0};
     SADCS_TRY(configureOnce(configured, [] {

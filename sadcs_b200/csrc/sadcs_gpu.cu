@@ -13,6 +13,7 @@
 #include <chrono>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <new>
@@ -58,6 +59,20 @@ double secondsSince(std::chrono::steady_clock::time_point start) {
 constexpr int64_t kMemoryReserve = int64_t(256) << 20;          // gpusa.h:82
 constexpr int64_t kMaxInt32Text = int64_t(INT32_MAX) - 1024;    // src/cpu/dcsort.h:21
 constexpr int64_t kMaxText = (int64_t(1) << 32) - 256;
+// Texts from this size on carry words through the class passes (in a one-text context, codes of at
+// most 2 bits): below it the packed text stays in the L2 and the final merge's record gathers hit
+// there (tuning).
+#ifndef SADCS_CARRY_MIN_BYTES
+#define SADCS_CARRY_MIN_BYTES (256ull << 20)
+#endif
+constexpr uint64_t kCarryMinBytes = SADCS_CARRY_MIN_BYTES;
+
+// The carry threshold: kCarryMinBytes, or the environment's SADCS_CARRY_MIN_BYTES (tests and tuning:
+// 0 makes every eligible construction carry words), read at each construction.
+uint64_t carryMinBytes() {
+    const char* v = std::getenv("SADCS_CARRY_MIN_BYTES");
+    return v && *v ? std::strtoull(v, nullptr, 0) : kCarryMinBytes;
+}
 constexpr uint32_t kMaxTexts = 1u << 20;
 
 // NVTX ranges of a construction's phases (upload, ranking, classes, merge) on the calling thread,
@@ -143,6 +158,7 @@ struct Layout {
     // class + merge region (overlaps the ranking region)
     size_t lists = 0, classScratch = 0, chain0 = 0, chain1 = 0, splitters = 0, rows = 0, sa = 0, bwt = 0,
            mergeCounter = 0;
+    size_t carried = 0;  // one word per list slot, through the class passes and the merge (0: none)
     size_t rankingEnd = 0, classEnd = 0, mergeEnd = 0, peak = 0;
 };
 
@@ -177,7 +193,9 @@ Extent extentBound(uint64_t total, uint32_t texts) {
     return e;
 }
 
-Layout planLayout(const Extent& x, bool internalSa, bool internalBwt) {
+// carry: room for the carried words (contexts of one text: their constructions carry words when the
+// codes take at most 2 bits).
+Layout planLayout(const Extent& x, bool internalSa, bool internalBwt, bool carry) {
     Layout L;
     size_t at = 0;
     auto take = [&at](size_t bytes) {
@@ -222,6 +240,11 @@ Layout planLayout(const Extent& x, bool internalSa, bool internalBwt) {
     L.sa = internalSa ? take(4 * x.outputs) : 0;
     L.bwt = internalBwt ? take(x.outputs) : 0;
     L.mergeEnd = at;
+    if (carry) {  // after both the class and the merge region: live through both
+        at = std::max(L.classEnd, L.mergeEnd);
+        L.carried = take(8 * x.outputs);
+        L.classEnd = L.mergeEnd = at;
+    }
     L.peak = std::max({L.rankingEnd, L.classEnd, L.mergeEnd});
     return L;
 }
@@ -291,6 +314,7 @@ struct sadcs_gpu_context {
     uint64_t capacity = 0;
     uint32_t maxTexts = 1;
     size_t slabBytes = 0;
+    bool carryRoom = false;  // the slab has room for carried words (one text)
     uint8_t* slab = nullptr;
     cudaStream_t stream = nullptr;
     uint32_t* hostWords = nullptr;  // page-locked: counters and the per-construction tables
@@ -350,8 +374,16 @@ int queryDevice(sadcs_gpu_device* device) {
     return SADCS_OK;
 }
 
+// Whether a context for (capacity, texts) has room for carried words: one text, and a capacity that
+// reaches the carry threshold (smaller contexts never carry, so they do not pay for the room).
+bool planCarry(uint64_t capacity, uint32_t texts) { return texts <= 1 && capacity >= carryMinBytes(); }
+
+size_t contextBytes(int64_t capacity, uint32_t texts, bool carry) {
+    return planLayout(extentBound(static_cast<uint64_t>(capacity), texts), true, true, carry).peak;
+}
+
 size_t contextBytes(int64_t capacity, uint32_t texts) {
-    return planLayout(extentBound(static_cast<uint64_t>(capacity), texts), true, true).peak;
+    return contextBytes(capacity, texts, planCarry(static_cast<uint64_t>(capacity), texts));
 }
 
 int createContext(int64_t capacity, uint32_t texts, sadcs_gpu_context** out) {
@@ -363,7 +395,8 @@ int createContext(int64_t capacity, uint32_t texts, sadcs_gpu_context** out) {
                  static_cast<long long>(capacity), texts, static_cast<long long>(kMaxText), kMaxTexts);
         return SADCS_FAILED;
     }
-    const size_t bytes = contextBytes(capacity, texts);
+    const bool carry = planCarry(static_cast<uint64_t>(capacity), texts);
+    const size_t bytes = contextBytes(capacity, texts, carry);
     if (static_cast<int64_t>(bytes) + kMemoryReserve > device.free_bytes) {
         setError("needs %lld MiB of device memory plus %lld MiB reserve, %lld MiB free",
                  static_cast<long long>(bytes >> 20), static_cast<long long>(kMemoryReserve >> 20),
@@ -378,6 +411,7 @@ int createContext(int64_t capacity, uint32_t texts, sadcs_gpu_context** out) {
     cudaGetDevice(&c->device);
     c->capacity = static_cast<uint64_t>(capacity);
     c->maxTexts = texts;
+    c->carryRoom = carry;
     c->slabBytes = bytes;
     // counters, then the host copy of the tables (without the block map, built on the device)
     c->hostWordCount = 64 + metaWords(texts, 0) + 2 * static_cast<size_t>(texts) + 64 + 256;
@@ -488,7 +522,7 @@ int construct(sadcs_gpu_context* c, const Batch& b, Io& io, cudaStream_t stream,
         return SADCS_NOT_ENOUGH_MEMORY;
     }
     const Layout L = planLayout(extentOf(b), io.wantSa && !io.outSa && !io.saPieces,
-                                io.wantBwt && !io.outBwt && !io.bwtPieces);
+                                io.wantBwt && !io.outBwt && !io.bwtPieces, c->carryRoom && b.count == 1);
     if (L.peak > c->slabBytes) {
         setError("internal: layout of %llu bytes exceeds the slab of %llu", static_cast<unsigned long long>(L.peak),
                  static_cast<unsigned long long>(c->slabBytes));
@@ -641,8 +675,12 @@ int construct(sadcs_gpu_context* c, const Batch& b, Io& io, cudaStream_t stream,
     uint32_t* lists = reinterpret_cast<uint32_t*>(slab + L.lists);
     uint32_t* classScratch = reinterpret_cast<uint32_t*>(slab + L.classScratch);
     uint64_t* const chains[2] = {reinterpret_cast<uint64_t*>(slab + L.chain0), reinterpret_cast<uint64_t*>(slab + L.chain1)};
+    // Carried words: on texts large enough that the final merge's record gathers leave the L2.
+    uint64_t* carried = L.carried && carriesWords(texts) && b.outputs >= carryMinBytes()
+                            ? reinterpret_cast<uint64_t*>(slab + L.carried)
+                            : nullptr;
     if ((error = sortClasses(J == 1 ? b.end[0] : b.end[J - 1], texts, ranks, static_cast<uint32_t>(b.slots), b.classes,
-                             classTables, lists, classScratch, chains, stream)) != cudaSuccess) {
+                             classTables, lists, classScratch, chains, carried, stream)) != cudaSuccess) {
         return failed("class sorts", error);
     }
     cudaEventRecord(c->events[2], stream);
@@ -669,7 +707,7 @@ int construct(sadcs_gpu_context* c, const Batch& b, Io& io, cudaStream_t stream,
                               reinterpret_cast<uint32_t*>(slab + L.splitters),
                               reinterpret_cast<MergeRow*>(slab + L.rows), sa, bwt,
                               reinterpret_cast<uint32_t*>(slab + L.mergeCounter), c->hostWords, stream,
-                              c->events[4], c->events[5], saPieces, bwtPieces)) != cudaSuccess) {
+                              c->events[4], c->events[5], saPieces, bwtPieces, carried)) != cudaSuccess) {
         return failed("merge", error);
     }
     cudaEventRecord(c->events[3], stream);
@@ -1411,7 +1449,7 @@ int sadcs_gpu_rank_sample(const uint8_t* text, int64_t n, uint32_t* ranks, sadcs
     Batch b;
     planBatch(&length, 1, b);
     return withContext(nullptr, length, 1, s, [&](sadcs_gpu_context* c) -> int {
-        const Layout L = planLayout(extentOf(b), false, false);
+        const Layout L = planLayout(extentOf(b), false, false, false);
         uint8_t* textBuffer = c->slab + L.text;
         uint32_t* rankBuffer = reinterpret_cast<uint32_t*>(c->slab + L.ranks);
         cudaError_t error;

@@ -86,9 +86,10 @@ bool takeInjectedFailure(sadcs_gpu_server* srv) {
     return false;
 }
 
-// Footprint of a construction: its planned peak on the device.
+// Footprint of a construction: its planned peak on the device (a one-text batch from the carry
+// threshold on with room for carried words).
 size_t footprintOf(const Batch& b) {
-    return planLayout(extentOf(b), true, true).peak;
+    return planLayout(extentOf(b), true, true, planCarry(b.outputs, b.count)).peak;
 }
 
 void serveBatch(sadcs_gpu_server* srv, sadcs_gpu_context& ctx, std::vector<ServerRequest*>& group, const Batch& b,
@@ -111,6 +112,8 @@ void serveBatch(sadcs_gpu_server* srv, sadcs_gpu_context& ctx, std::vector<Serve
         ctx.slabBytes = footprint;
         ctx.capacity = b.outputs;
         ctx.maxTexts = b.count;
+        // room for carried words if the footprint was planned with it
+        ctx.carryRoom = b.count <= 1 && planLayout(extentOf(b), true, true, true).peak <= footprint;
         Io io;
         io.wantSa = true;
         io.wantBwt = true;

@@ -48,7 +48,10 @@ extern "C" int plan_check(const uint64_t* lengths, uint32_t count, uint64_t capa
     }
     for (int sa = 0; sa < 2; sa++) {
         for (int bwt = 0; bwt < 2; bwt++) {
-            const size_t need = planLayout(a, sa, bwt).peak, have = planLayout(x, sa, bwt).peak;
+            // a one-text context from the carry threshold on plans room for carried words; its
+            // constructions use it
+            const bool carry = planCarry(capacity, texts);
+            const size_t need = planLayout(a, sa, bwt, carry).peak, have = planLayout(x, sa, bwt, carry).peak;
             if (need > have) {
                 detail[0] = 2 * sa + bwt;
                 detail[1] = static_cast<int64_t>(need);
@@ -57,7 +60,9 @@ extern "C" int plan_check(const uint64_t* lengths, uint32_t count, uint64_t capa
             }
         }
     }
-    if (planLayout(a, true, true).peak > contextBytes(static_cast<int64_t>(capacity), texts)) return 21;
+    if (planLayout(a, true, true, planCarry(capacity, texts)).peak > contextBytes(static_cast<int64_t>(capacity), texts)) {
+        return 21;
+    }
     return 0;
 }
 
@@ -65,5 +70,5 @@ extern "C" int plan_check(const uint64_t* lengths, uint32_t count, uint64_t capa
 extern "C" uint64_t plan_peak(const uint64_t* lengths, uint32_t count) {
     Batch b;
     if (!planBatch(lengths, count, b)) return 0;
-    return planLayout(extentOf(b), true, true).peak;
+    return planLayout(extentOf(b), true, true, planCarry(b.outputs, count)).peak;
 }

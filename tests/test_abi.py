@@ -54,9 +54,10 @@ def test_required_bytes_plan():
         need = sa.required_bytes(n)
         assert need >= previous
         previous = need
-    # SA + BWT from one construction: text, packed codes, ranks, lists, SA, BWT and small arrays.
-    per_byte = sa.required_bytes(256 << 20) / (256 << 20)
-    assert 10.0 < per_byte < 11.5
+    # SA + BWT from one construction: text, packed codes, ranks, lists, SA, BWT and small arrays;
+    # from the carry threshold on, one word per input byte more for the carried code words.
+    assert 10.0 < sa.required_bytes(64 << 20) / (64 << 20) < 11.5
+    assert 18.0 < sa.required_bytes(3 << 30) / (3 << 30) < 19.5
     assert sa.memory_reserve() == 256 << 20
 
 

@@ -114,6 +114,34 @@ def test_large(kind):
     _check_ranks(text, name=f"large {kind}")
 
 
+def test_carried_words(monkeypatch):
+    """Constructions that hand each suffix's first code word from class to class instead of the
+    final merge gathering it (one text, codes of at most 2 bits; on their own only from 256 MiB on),
+    forced on small texts: the SA, BWT and primary index stay the oracle's. Texts of wider codes take
+    the gathering path under the same setting."""
+    monkeypatch.setenv("SADCS_CARRY_MIN_BYTES", "0")
+    rng = W.SplitMix(21)
+    for word in (b"a", b"ab", b"ba", b"banana", b"mississippi", b"acgt" * 9, b"abracadabra"):
+        _check(np.frombuffer(word, np.uint8), name=f"carry {word!r}")
+    for n in range(0, 81):
+        _check(W.run_text(n), name=f"carry run n={n}")
+        _check(W.random_text(rng, n, 2), name=f"carry sigma=2 n={n}")
+        _check(W.random_text(rng, n, 4), name=f"carry sigma=4 n={n}")
+    _check(W.fibonacci_text(5000), name="carry fibonacci")
+    _check(W.thue_morse_text(4096), name="carry thue-morse")
+    _check(np.zeros(1000, np.uint8), name="carry zeros")
+    for i in range(6):
+        n = 1 + int(rng.below(40000)[0])
+        _check(W.random_text(rng, n, 2 + i % 3), name=f"carry sigma={2 + i % 3} #{i}")
+    _check(W.run_text(LARGE), name="carry large run")
+    _check(W.fibonacci_text(LARGE), name="carry large fibonacci")
+    _check(W.random_text(rng, LARGE, 4), name="carry large sigma=4")
+    _check(W.genome_text(LARGE, seed=5), name="carry genome-like 4M")
+    with sa.Context(20_000_000) as ctx:
+        _check(W.random_text(rng, 20_000_000, 4), context=ctx, name="carry context sigma=4 20M")
+        _check(W.random_text(rng, LARGE, 3), context=ctx, name="carry context sigma=3")
+
+
 def test_context_reuse_and_refusal():
     """selftest.cpp:505-541: one context, largest input first, empties, a refusal, then reuse."""
     rng = W.SplitMix(3)
