@@ -117,17 +117,23 @@ __device__ __forceinline__ uint64_t carriedWord(const uint64_t* __restrict__ pac
 // the slice; one run per slice and block); classScatterPairs then walks the pairs slice by slice,
 // and each slice's writes stay within the list's L2-sized slice.
 constexpr uint32_t kSampleSliceShift = 23;  // 8M ranks = 32 MB of the list per slice
+#ifndef SADCS_CARRY_SLICE_SHIFT
+#define SADCS_CARRY_SLICE_SHIFT 22  // with carried words: 4M ranks = 16 + 32 MB per slice (tuning)
+#endif
+constexpr uint32_t kCarrySampleSliceShift = SADCS_CARRY_SLICE_SHIFT;
 constexpr uint32_t kMaxSampleSlices = kMaxSlices;
 
-// The slice width (as a shift) for `live` samples: at least 8M ranks, at most kMaxSampleSlices slices.
-inline uint32_t sampleSliceShift(uint64_t live) {
-    uint32_t shift = kSampleSliceShift;
+// The slice width (as a shift) for `live` samples: at least 8M ranks (4M with carried words), at
+// most kMaxSampleSlices slices.
+inline uint32_t sampleSliceShift(uint64_t live, bool carry) {
+    uint32_t shift = carry ? kCarrySampleSliceShift : kSampleSliceShift;
     while ((live >> shift) >= kMaxSampleSlices) shift++;
     return shift;
 }
 
 // fill[k] (zeroed by the caller) counts the pairs placed in slice k so far. kCarry: words[x] = the
-// carried word of the sample in pairs[x] (the samples are read in text order, so are their words).
+// carried word of the sample in pairs[x] (a block's samples are consecutive in the text, so their
+// words are one short stretch of the code stream).
 template <bool kCarry>
 __global__ void __launch_bounds__(kSliceThreads) classPartitionSample(const uint32_t* __restrict__ ranks,
                                                                      uint32_t slots, uint32_t live, uint32_t shift,
@@ -135,26 +141,26 @@ __global__ void __launch_bounds__(kSliceThreads) classPartitionSample(const uint
                                                                      uint64_t* __restrict__ pairs,
                                                                      uint64_t* __restrict__ words) {
     __shared__ SliceStage stage;
-    uint64_t v[kSliceItems], w[kSliceItems];
+    uint64_t v[kSliceItems];
     const uint64_t first = static_cast<uint64_t>(blockIdx.x) * kSliceTile + threadIdx.x;
 #pragma unroll
     for (int j = 0; j < kSliceItems; j++) {
         const uint64_t t = first + static_cast<uint64_t>(j) * kSliceThreads;
         v[j] = kNoPair;
-        w[j] = 0;
         if (t < slots) {
             const uint32_t rank = __ldcs(ranks + t);  // streamed: read once
             const uint32_t q = samplePosition(static_cast<uint32_t>(t));
             // a live sample (not past the end or between texts)
-            if (q < texts.endOf(q) && rank < live) {
-                v[j] = (static_cast<uint64_t>(rank) << 32) | q;
-                if constexpr (kCarry) w[j] = carriedWord(texts.packed, q, texts.bits);
-            }
+            if (q < texts.endOf(q) && rank < live) v[j] = (static_cast<uint64_t>(rank) << 32) | q;
         }
     }
     if constexpr (kCarry) {
         __shared__ SliceCompanion companion;
-        writeSliceMajor(stage, v, shift, fill, pairs, live, &companion, &w, words);
+        const uint64_t* packed = texts.packed;
+        const uint32_t bits = texts.bits;
+        writeSliceMajor(stage, v, shift, fill, pairs, live, &companion,
+                        [packed, bits](uint64_t pair) { return carriedWord(packed, static_cast<uint32_t>(pair), bits); },
+                        words);
     } else {
         writeSliceMajor(stage, v, shift, fill, pairs, live);
     }
@@ -243,11 +249,20 @@ struct ClassLoader {
     __device__ __forceinline__ uint8_t carryTag(Chain key) const {
         return static_cast<uint8_t>((static_cast<uint32_t>(key) >> texts.bits) & ((1u << texts.bits) - 1));
     }
-    // carried(p - 1) from carried(p) (the text's end: from the code stream).
-    __device__ __forceinline__ uint64_t carry(uint32_t j, uint32_t, uint32_t k, uint32_t tag) const {
+    // carried(p) for the element p (the text's end: carried(end - 1) itself, from the code stream),
+    // then carried(p - 1) from it and the code of T[p - 2].
+    __device__ __forceinline__ uint64_t carrySource(uint32_t j, uint32_t, uint32_t k) const {
         if (k == 0) return carriedWord(texts.packed, texts.endOfText(j) - 1, texts.bits);
-        const uint64_t from = carried[__ldg(prevOffset + j) + k - 1];
-        return (static_cast<uint64_t>(tag) << (64 - texts.bits)) | (from >> texts.bits);
+        return carried[__ldg(prevOffset + j) + k - 1];
+    }
+    __device__ __forceinline__ const uint64_t* carrySourceAt(uint32_t j, uint32_t, uint32_t k) const {
+        return k == 0 ? nullptr : carried + __ldg(prevOffset + j) + k - 1;
+    }
+    __device__ __forceinline__ uint64_t carryCombine(uint32_t tag, uint64_t source) const {
+        return (static_cast<uint64_t>(tag) << (64 - texts.bits)) | (source >> texts.bits);
+    }
+    __device__ __forceinline__ uint64_t carryWord(uint32_t k, uint32_t tag, uint64_t source) const {
+        return k == 0 ? source : carryCombine(tag, source);
     }
 };
 
@@ -365,10 +380,10 @@ inline cudaError_t sortClasses(uint32_t total, const TextSet& texts, const uint3
     // (with carried words: the pairs' words in chain buffer 1, also free until pass 1)
     if (carried) {
         SADCS_TRY(launch(classPartitionSample<true>, ceilDiv(slots, kSliceTile), kSliceThreads, 0, stream, ranks, slots,
-                         live, sampleSliceShift(live), texts, fill, chains[0], chains[1]));
+                         live, sampleSliceShift(live, true), texts, fill, chains[0], chains[1]));
     } else {
         SADCS_TRY(launch(classPartitionSample<false>, ceilDiv(slots, kSliceTile), kSliceThreads, 0, stream, ranks,
-                         slots, live, sampleSliceShift(live), texts, fill, chains[0], nullptr));
+                         slots, live, sampleSliceShift(live, false), texts, fill, chains[0], nullptr));
     }
     SADCS_TRY(launch(classScatterPairs, ceilDiv(live, 256), 256, 0, stream, chains[0], live, lists, carried,
                      chains[1]));

@@ -226,6 +226,22 @@ inline cudaError_t configureOnce(std::atomic<uint64_t>& configured, Set set) {
     return cudaSuccess;
 }
 
+// Asynchronous copies from global to shared memory (completed by cpAsyncWaitAll in the issuing
+// thread, then visible to the block after a barrier).
+__device__ __forceinline__ void cpAsync8(void* sharedDst, const void* globalSrc) {
+    const uint32_t dst = static_cast<uint32_t>(__cvta_generic_to_shared(sharedDst));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(globalSrc) : "memory");
+}
+
+__device__ __forceinline__ void cpAsync4(void* sharedDst, const void* globalSrc) {
+    const uint32_t dst = static_cast<uint32_t>(__cvta_generic_to_shared(sharedDst));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(dst), "l"(globalSrc) : "memory");
+}
+
+__device__ __forceinline__ void cpAsyncWaitAll() {
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
+
 }  // namespace sadcs
 
 #define SADCS_TRY(call)                                 \

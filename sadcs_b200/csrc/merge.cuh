@@ -163,20 +163,6 @@ __device__ __forceinline__ bool lessRecord(const MergeRecord& a, const MergeReco
     return a.rank[tb.slot[i % kV][k]] < b.rank[tb.slot[j % kV][k]];
 }
 
-__device__ __forceinline__ void cpAsync8(void* sharedDst, const void* globalSrc) {
-    const uint32_t dst = static_cast<uint32_t>(__cvta_generic_to_shared(sharedDst));
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(globalSrc) : "memory");
-}
-
-__device__ __forceinline__ void cpAsync4(void* sharedDst, const void* globalSrc) {
-    const uint32_t dst = static_cast<uint32_t>(__cvta_generic_to_shared(sharedDst));
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(dst), "l"(globalSrc) : "memory");
-}
-
-__device__ __forceinline__ void cpAsyncWaitAll() {
-    asm volatile("cp.async.wait_all;\n" ::: "memory");
-}
-
 struct MergeTileInfo {
     uint32_t seg[kClasses + 1];
     uint32_t win[kClasses];

@@ -169,7 +169,9 @@ cudaError_t deviceScan(const uint32_t* in, uint32_t* out, uint32_t count, uint32
 constexpr int kSliceThreads = 256;
 constexpr int kSliceItems = 16;
 constexpr uint32_t kSliceTile = kSliceThreads * kSliceItems;
-constexpr uint32_t kMaxSlices = 128;
+constexpr uint32_t kMaxSlices = 256;
+constexpr int kSlicesPerLane = kMaxSlices / 32;
+static_assert(kMaxSlices <= kSliceThreads, "one thread per slice reserves the runs");
 constexpr uint64_t kNoPair = ~uint64_t(0);
 
 struct SliceStage {
@@ -185,15 +187,21 @@ struct SliceCompanion {
     uint8_t slice[kSliceTile];
 };
 
+// No companion words.
+struct NoCompanion {
+    __device__ __forceinline__ uint64_t operator()(uint64_t) const { return 0; }
+};
+
 // All threads of the block, each with its kSliceItems pairs (kNoPair where it has none, and for
 // any pair whose slice is not below kMaxSlices). fill[k] (zeroed by the caller before the launch)
-// counts the pairs placed in slice k; capacity bounds the pair array. With a companion (cs, w,
-// dstW non-null), w[j] is written to dstW at the place v[j] goes to in dst.
+// counts the pairs placed in slice k; capacity bounds the pair array. With a companion (cs and dstW
+// non-null), wordOf(v[j]) is written to dstW at the place v[j] goes to in dst (computed after the
+// pairs are out, so that the words are not held in registers meanwhile).
+template <class WordOf = NoCompanion>
 __device__ __forceinline__ void writeSliceMajor(SliceStage& st, const uint64_t (&v)[kSliceItems], uint32_t shift,
                                                 uint32_t* __restrict__ fill, uint64_t* __restrict__ dst,
                                                 uint64_t capacity, SliceCompanion* cs = nullptr,
-                                                const uint64_t (*w)[kSliceItems] = nullptr,
-                                                uint64_t* __restrict__ dstW = nullptr) {
+                                                WordOf wordOf = WordOf(), uint64_t* __restrict__ dstW = nullptr) {
     for (uint32_t i = threadIdx.x; i < kMaxSlices; i += kSliceThreads) st.count[i] = 0;
     __syncthreads();
     uint32_t local[kSliceItems];
@@ -202,12 +210,12 @@ __device__ __forceinline__ void writeSliceMajor(SliceStage& st, const uint64_t (
         local[j] = v[j] == kNoPair ? 0 : atomicAdd(&st.count[static_cast<uint32_t>(v[j] >> 32) >> shift], 1u);
     }
     __syncthreads();
-    if (threadIdx.x < 32) {  // exclusive scan of the counts, 4 slices per lane
+    if (threadIdx.x < 32) {  // exclusive scan of the counts, kSlicesPerLane slices per lane
         const uint32_t lane = threadIdx.x;
-        uint32_t c[4], sum = 0;
+        uint32_t c[kSlicesPerLane], sum = 0;
 #pragma unroll
-        for (int q = 0; q < 4; q++) {
-            c[q] = st.count[4 * lane + q];
+        for (int q = 0; q < kSlicesPerLane; q++) {
+            c[q] = st.count[kSlicesPerLane * lane + q];
             sum += c[q];
         }
         uint32_t inclusive = sum;
@@ -218,8 +226,8 @@ __device__ __forceinline__ void writeSliceMajor(SliceStage& st, const uint64_t (
         }
         uint32_t at = inclusive - sum;
 #pragma unroll
-        for (int q = 0; q < 4; q++) {
-            st.offset[4 * lane + q] = at;
+        for (int q = 0; q < kSlicesPerLane; q++) {
+            st.offset[kSlicesPerLane * lane + q] = at;
             at += c[q];
         }
     }
@@ -245,7 +253,7 @@ __device__ __forceinline__ void writeSliceMajor(SliceStage& st, const uint64_t (
         __syncthreads();
 #pragma unroll
         for (int j = 0; j < kSliceItems; j++) {
-            if (v[j] != kNoPair) st.pairs[st.offset[static_cast<uint32_t>(v[j] >> 32) >> shift] + local[j]] = (*w)[j];
+            if (v[j] != kNoPair) st.pairs[st.offset[static_cast<uint32_t>(v[j] >> 32) >> shift] + local[j]] = wordOf(v[j]);
         }
         __syncthreads();
         for (uint32_t i = threadIdx.x; i < total; i += kSliceThreads) {
@@ -284,12 +292,15 @@ constexpr uint32_t kMaxSortCount = kStatusValue;
 constexpr long long kLookbackLimitCycles = 4000000000ll;
 
 // Shared memory of radixOnesweep for a key of keyBytes bytes: one staging buffer that holds the
-// tile's keys, then its values, then (carry) its 64-bit carried words; the digit of every staged
-// slot, (carry) a tag byte per slot, and the counting tables.
-constexpr size_t radixSharedBytes(size_t keyBytes, bool carry = false) {
-    const size_t stage = carry ? 8 : (keyBytes > 4 ? keyBytes : 4);
-    return kSortTile * stage + kSortTile * (carry ? 2 : 1) + (kSortWarps * 256 + 256 + 256 + 32) * 4 + 64;
+// tile's keys, then its values, then (carry mode 0) its 64-bit carried words; the digit of every
+// staged slot, (carry) a tag byte per slot, the counting tables, and (carry mode 3) a buffer of the
+// carried words' sources by slot. The shared memory a block does not take is L1.
+constexpr size_t radixSharedBytes(size_t keyBytes, bool carry = false, int carryMode = 0) {
+    const size_t stage = carry && carryMode == 0 ? 8 : (keyBytes > 4 ? keyBytes : 4);
+    return kSortTile * stage + kSortTile * (carry ? 2 : 1) + (kSortWarps * 256 + 256 + 256 + 32) * 4 +
+           (carry && carryMode == 3 ? 8 * kSortTile : 0) + 64;
 }
+constexpr uint8_t kCarryAsIs = 0xFF;  // tag of a slot whose source is its carried word already
 
 // Segments of a pass: element ranges sorted independently, each from its own digit bases, with
 // tiles that never span two segments. The one-segment case is the plain sort.
@@ -343,8 +354,18 @@ struct SortTilesPerSm<Loader, std::void_t<decltype(Loader::kTilesPerSm)>> {
 };
 
 // A loader may carry a 64-bit word with every element (kCarry): it gives a tag byte from the key
-// (carryTag), staged while the key is in registers, and after the look-back the element's carried
-// word from its index and that tag (carry); the storer writes it (storeCarry).
+// (carryTag), staged while the key is in registers, a source word read by the element's index
+// (carrySource), and the element's carried word from the two (carryWord); the storer writes it
+// (storeCarry). SADCS_CARRY_MODE: 0 reads the sources after the look-back and stages the words by
+// slot (whole-run stores); 1 reads them after the look-back and stores each from its thread (a
+// warp's stores fall into one run per digit); 2 as 1, but with the sources read before the
+// look-back, with the values; 3 copies the sources asynchronously into a slot-ordered buffer of
+// their own before the look-back (carrySourceAt; no registers held), then stores in runs (tuning).
+// Measured on the 3 GiB genome-like text (class phase): mode 0 91.3 ms, 1 82.8, 2 93.8 (3 tiles per
+// SM: its registers spill at 4), 3 95.6 (3 tiles per SM: its shared memory).
+#ifndef SADCS_CARRY_MODE
+#define SADCS_CARRY_MODE 1
+#endif
 template <class Loader, class = void>
 struct LoaderCarries {
     static constexpr bool value = false;
@@ -363,7 +384,10 @@ __global__ void __launch_bounds__(kSortThreads, SortTilesPerSm<Loader>::value) r
                                                                  long long lookbackLimit) {
     extern __shared__ __align__(16) unsigned char smem[];
     constexpr bool kCarry = LoaderCarries<Loader>::value;
-    constexpr size_t kStageBytes = kSortTile * (kCarry ? 8 : (sizeof(Key) > 4 ? sizeof(Key) : 4));
+    constexpr bool kStageCarry = kCarry && SADCS_CARRY_MODE == 0;
+    constexpr bool kEarlyCarry = kCarry && SADCS_CARRY_MODE == 2;
+    constexpr bool kPrefetchCarry = kCarry && SADCS_CARRY_MODE == 3;
+    constexpr size_t kStageBytes = kSortTile * (kStageCarry ? 8 : (sizeof(Key) > 4 ? sizeof(Key) : 4));
     Key* sKeys = reinterpret_cast<Key*>(smem);
     uint32_t* sVals = reinterpret_cast<uint32_t*>(smem);  // the same buffer, after the keys are out
     uint64_t* sCarry = reinterpret_cast<uint64_t*>(smem);  // and after the values
@@ -373,6 +397,7 @@ __global__ void __launch_bounds__(kSortThreads, SortTilesPerSm<Loader>::value) r
     uint32_t* digitStart = warpCount + kSortWarps * 256;
     uint32_t* digitGlobal = digitStart + 256;
     uint32_t* warpTotals = digitGlobal + 256;
+    uint64_t* sSource = reinterpret_cast<uint64_t*>(warpTotals + 32);  // prefetch mode only (16-byte aligned)
     __shared__ uint32_t sTile;
     __shared__ int sFailed;
 
@@ -439,10 +464,12 @@ __global__ void __launch_bounds__(kSortThreads, SortTilesPerSm<Loader>::value) r
     // Stage the keys (and every slot's digit) by digit before the look-back, so that the keys leave
     // the registers, and start the value loads, which complete while the look-back waits.
     uint32_t vals[kSortItems];
+    uint64_t sources[kCarry ? kSortItems : 1];
 #pragma unroll
     for (int j = 0; j < kSortItems; j++) {
         const uint32_t dj = rankDigit[j] & 0x1FF;
         vals[j] = 0;
+        if constexpr (kEarlyCarry) sources[j] = 0;
         if (dj != kNoDigit) {
             const uint32_t slot = digitStart[dj] + warpCount[warp * 256 + dj] + (rankDigit[j] >> 9);
             if constexpr (Storer::kKeys) sKeys[slot] = keys[j];
@@ -451,6 +478,18 @@ __global__ void __launch_bounds__(kSortThreads, SortTilesPerSm<Loader>::value) r
             rankDigit[j] = slot;  // from here on: the item's staged slot
             const uint64_t i = warpBase + j * 32 + lane;
             vals[j] = ld.value(segment, segBegin + static_cast<uint32_t>(i), static_cast<uint32_t>(i));
+            if constexpr (kEarlyCarry) {
+                sources[j] = ld.carrySource(segment, segBegin + static_cast<uint32_t>(i), static_cast<uint32_t>(i));
+            }
+            if constexpr (kPrefetchCarry) {
+                const uint64_t* from = ld.carrySourceAt(segment, segBegin + static_cast<uint32_t>(i), static_cast<uint32_t>(i));
+                if (from) {
+                    cpAsync8(sSource + slot, from);
+                } else {
+                    sSource[slot] = ld.carrySource(segment, segBegin + static_cast<uint32_t>(i), static_cast<uint32_t>(i));
+                    sTag[slot] = kCarryAsIs;
+                }
+            }
         } else {
             rankDigit[j] = 0xFFFFFFFFu;
         }
@@ -504,6 +543,7 @@ __global__ void __launch_bounds__(kSortThreads, SortTilesPerSm<Loader>::value) r
     digitGlobal[d] = digitBase[static_cast<size_t>(segment) * 256 + d] + exclusive;
     __syncthreads();
     if (sFailed) {
+        if constexpr (kPrefetchCarry) cpAsyncWaitAll();  // no copy into shared memory outlives the block
         if (threadIdx.x == 0) atomicExch(error, 1u);
         return;
     }
@@ -525,27 +565,55 @@ __global__ void __launch_bounds__(kSortThreads, SortTilesPerSm<Loader>::value) r
         const uint32_t dj = sDig[i];
         st.storeValue(segment, digitGlobal[dj] + i - digitStart[dj], sVals[i]);
     }
-    if constexpr (kCarry) {
-        // The carried words: read in element order (every read in flight), staged by slot, written.
-        uint64_t carried[kSortItems];
-#pragma unroll
-        for (int j = 0; j < kSortItems; j++) {
-            const uint64_t i = warpBase + j * 32 + lane;
-            carried[j] = 0;
-            if (rankDigit[j] != 0xFFFFFFFFu) {
-                carried[j] = ld.carry(segment, segBegin + static_cast<uint32_t>(i), static_cast<uint32_t>(i),
-                                      sTag[rankDigit[j]]);
-            }
-        }
-        __syncthreads();  // the values are out of the staging buffer
-#pragma unroll
-        for (int j = 0; j < kSortItems; j++) {
-            if (rankDigit[j] != 0xFFFFFFFFu) sCarry[rankDigit[j]] = carried[j];
-        }
+    if constexpr (kPrefetchCarry) {
+        cpAsyncWaitAll();
         __syncthreads();
         for (uint32_t i = threadIdx.x; i < tileTotal; i += kSortThreads) {
             const uint32_t dj = sDig[i];
-            st.storeCarry(segment, digitGlobal[dj] + i - digitStart[dj], sCarry[i]);
+            const uint8_t tag = sTag[i];
+            const uint64_t source = sSource[i];
+            st.storeCarry(segment, digitGlobal[dj] + i - digitStart[dj],
+                          tag == kCarryAsIs ? source : ld.carryCombine(tag, source));
+        }
+    } else if constexpr (kCarry) {
+        // The carried words: sources read in element order (every read in flight), then each word
+        // staged by slot and written in runs (mode 0) or written from its thread (modes 1, 2).
+        if constexpr (!kEarlyCarry) {
+#pragma unroll
+            for (int j = 0; j < kSortItems; j++) {
+                const uint64_t i = warpBase + j * 32 + lane;
+                sources[j] = 0;
+                if (rankDigit[j] != 0xFFFFFFFFu) {
+                    sources[j] = ld.carrySource(segment, segBegin + static_cast<uint32_t>(i), static_cast<uint32_t>(i));
+                }
+            }
+        }
+        if constexpr (kStageCarry) {
+            __syncthreads();  // the values are out of the staging buffer
+#pragma unroll
+            for (int j = 0; j < kSortItems; j++) {
+                const uint32_t slot = rankDigit[j];
+                if (slot != 0xFFFFFFFFu) {
+                    const uint64_t i = warpBase + j * 32 + lane;
+                    sCarry[slot] = ld.carryWord(static_cast<uint32_t>(i), sTag[slot], sources[j]);
+                }
+            }
+            __syncthreads();
+            for (uint32_t i = threadIdx.x; i < tileTotal; i += kSortThreads) {
+                const uint32_t dj = sDig[i];
+                st.storeCarry(segment, digitGlobal[dj] + i - digitStart[dj], sCarry[i]);
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < kSortItems; j++) {
+                const uint32_t slot = rankDigit[j];
+                if (slot != 0xFFFFFFFFu) {
+                    const uint64_t i = warpBase + j * 32 + lane;
+                    const uint32_t dj = sDig[slot];
+                    st.storeCarry(segment, digitGlobal[dj] + slot - digitStart[dj],
+                                  ld.carryWord(static_cast<uint32_t>(i), sTag[slot], sources[j]));
+                }
+            }
         }
     }
 }
@@ -691,7 +759,7 @@ cudaError_t radixOnesweepPass(const Loader& ld, const Storer& st, const Segments
     SADCS_TRY(cudaMemsetAsync(scratch.status, 0, static_cast<size_t>(tiles + skipTiles) * 256 * 4, stream));
     SADCS_TRY(cudaMemsetAsync(scratch.control, 0, 4, stream));
     if (skipTiles) SADCS_TRY(cudaMemsetAsync(scratch.control, static_cast<int>(skipTiles), 1, stream));
-    constexpr size_t shared = radixSharedBytes(sizeof(Key), LoaderCarries<Loader>::value);
+    constexpr size_t shared = radixSharedBytes(sizeof(Key), LoaderCarries<Loader>::value, SADCS_CARRY_MODE);
     // The opt-in above 48 KiB of dynamic shared memory is per function and per device.
     static std::atomic<uint64_t> configured{0};
     SADCS_TRY(configureOnce(configured, [] {

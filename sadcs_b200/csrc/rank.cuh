@@ -386,7 +386,10 @@ __global__ void __launch_bounds__(kRefineThreads) rankRefineApply(const uint32_t
 // writes each sample at most once, so slice k of the pair array has room for all of its pairs),
 // and rankScatterPairs writes the slices one after another, each within an L2-sized part of the
 // rank array.
-constexpr uint32_t kRankSliceShift = 23;  // 8M samples = 32 MB of the rank array per slice
+#ifndef SADCS_RANK_SLICE_SHIFT
+#define SADCS_RANK_SLICE_SHIFT 23  // 8M samples = 32 MB of the rank array per slice (tuning)
+#endif
+constexpr uint32_t kRankSliceShift = SADCS_RANK_SLICE_SHIFT;
 constexpr uint32_t kMaxRankSlices = kMaxSlices;
 constexpr int kPairThreads = 256;
 constexpr int kPairItems = 8;
