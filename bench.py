@@ -501,7 +501,7 @@ def run_ours(args, world, rank, local) -> None:
         roofline["traffic_source"] = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the final merge per input "
                                       "byte, captured on %s (profiles/traffic.json), times n%s" % (
                                           traffic[1], "" if traffic[1] == args.workload else
-                                          ": scaled to this size, a lower bound (less of the gathers hit L2)"))
+                                          ": scaled to this size, a lower bound (the tie-breaking rank reads hit L2 less)"))
     line = {"metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms_max, 3), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u8", "data": "synthetic",

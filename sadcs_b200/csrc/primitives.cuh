@@ -366,6 +366,12 @@ struct SortTilesPerSm<Loader, std::void_t<decltype(Loader::kTilesPerSm)>> {
 #ifndef SADCS_CARRY_MODE
 #define SADCS_CARRY_MODE 1
 #endif
+// Carrying passes in mode 1 store their values from the threads too, beside the words (a warp's
+// stores fall into one run per digit: few digits in the carrying passes), without staging them by
+// slot (tuning).
+#ifndef SADCS_CARRY_DIRECT_VALUES
+#define SADCS_CARRY_DIRECT_VALUES 0
+#endif
 template <class Loader, class = void>
 struct LoaderCarries {
     static constexpr bool value = false;
@@ -387,6 +393,7 @@ __global__ void __launch_bounds__(kSortThreads, SortTilesPerSm<Loader>::value) r
     constexpr bool kStageCarry = kCarry && SADCS_CARRY_MODE == 0;
     constexpr bool kEarlyCarry = kCarry && SADCS_CARRY_MODE == 2;
     constexpr bool kPrefetchCarry = kCarry && SADCS_CARRY_MODE == 3;
+    constexpr bool kDirectValues = kCarry && SADCS_CARRY_MODE == 1 && SADCS_CARRY_DIRECT_VALUES;
     constexpr size_t kStageBytes = kSortTile * (kStageCarry ? 8 : (sizeof(Key) > 4 ? sizeof(Key) : 4));
     Key* sKeys = reinterpret_cast<Key*>(smem);
     uint32_t* sVals = reinterpret_cast<uint32_t*>(smem);  // the same buffer, after the keys are out
@@ -548,6 +555,36 @@ __global__ void __launch_bounds__(kSortThreads, SortTilesPerSm<Loader>::value) r
         return;
     }
 
+    if constexpr (kDirectValues) {
+        // Sources of the carried words first (every read in flight), then the keys in runs and each
+        // item's value and word from its thread.
+#pragma unroll
+        for (int j = 0; j < kSortItems; j++) {
+            const uint64_t i = warpBase + j * 32 + lane;
+            sources[j] = 0;
+            if (rankDigit[j] != 0xFFFFFFFFu) {
+                sources[j] = ld.carrySource(segment, segBegin + static_cast<uint32_t>(i), static_cast<uint32_t>(i));
+            }
+        }
+        if constexpr (Storer::kKeys) {
+            for (uint32_t i = threadIdx.x; i < tileTotal; i += kSortThreads) {
+                const uint32_t dj = sDig[i];
+                st.storeKey(segment, digitGlobal[dj] + i - digitStart[dj], sKeys[i]);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < kSortItems; j++) {
+            const uint32_t slot = rankDigit[j];
+            if (slot != 0xFFFFFFFFu) {
+                const uint64_t i = warpBase + j * 32 + lane;
+                const uint32_t dj = sDig[slot];
+                const uint32_t pos = digitGlobal[dj] + slot - digitStart[dj];
+                st.storeValue(segment, pos, vals[j]);
+                st.storeCarry(segment, pos, ld.carryWord(static_cast<uint32_t>(i), sTag[slot], sources[j]));
+            }
+        }
+        return;
+    }
     if constexpr (Storer::kKeys) {
         for (uint32_t i = threadIdx.x; i < tileTotal; i += kSortThreads) {
             const uint32_t dj = sDig[i];

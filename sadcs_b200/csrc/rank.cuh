@@ -387,7 +387,7 @@ __global__ void __launch_bounds__(kRefineThreads) rankRefineApply(const uint32_t
 // and rankScatterPairs writes the slices one after another, each within an L2-sized part of the
 // rank array.
 #ifndef SADCS_RANK_SLICE_SHIFT
-#define SADCS_RANK_SLICE_SHIFT 23  // 8M samples = 32 MB of the rank array per slice (tuning)
+#define SADCS_RANK_SLICE_SHIFT 22  // 4M samples = 16 MB of the rank array per slice (tuning: 0.6 ms less ranking than 8M at 3 GiB)
 #endif
 constexpr uint32_t kRankSliceShift = SADCS_RANK_SLICE_SHIFT;
 constexpr uint32_t kMaxRankSlices = kMaxSlices;
