@@ -19,6 +19,9 @@
 // writes the elements between s_lo and s_hi (the last level: SA and BWT; upper levels: rows).
 #pragma once
 
+#include <algorithm>
+#include <cstring>
+
 #include "alphabet.cuh"
 #include "common.cuh"
 
@@ -65,6 +68,7 @@ struct __align__(16) MergeRow {
     uint32_t list;
     uint32_t c[kClasses];
 };
+static_assert(sizeof(MergeRow) == 32, "a row is 8 words");
 
 // A suffix for single comparisons in registers (the searches of mergeSuffixZeroRows): w0, w1 = 128
 // bits of the code stream from pos; end: the end of pos's text (texts are ordered by it); text: its
@@ -97,6 +101,7 @@ struct MergeArgs {
     uint8_t* const* bwtTexts;  // level 0, optional, in place of bwt: one output array per text
     uint32_t* error;         // set nonzero if a window set exceeds the capacity (never, by construction)
     const uint64_t* carried;  // level 0, optional: every list slot's carried word (one text, 1-word records)
+    uint32_t tileOffset;      // tiles of this launch start here (a level launched in pieces)
 };
 
 // The top `bits` bits set (bits <= 64).
@@ -189,7 +194,7 @@ __device__ __forceinline__ void planTileWindows(const MergeArgs& a, uint32_t cap
     if (!a.rowsIn) {
         if (b < kClasses) e = st[b + 1] - st[b];
     } else {
-        const MergeRow* lo = a.rowsIn + blockIdx.x;
+        const MergeRow* lo = a.rowsIn + a.tileOffset + blockIdx.x;
         const MergeRow* hi = lo + 1;
         loList = lo->list;
         hiList = hi->list;
@@ -343,6 +348,49 @@ inline MergePlan planMerge(const uint32_t* classStart, uint32_t r) {
 template <bool kFinal>
 inline cudaError_t launchTree(const MergeArgs& args, uint32_t tiles, cudaStream_t stream);
 
+// The download of the outputs to page-locked host buffers while the last level runs: the level is
+// launched in `chunks` pieces of tiles, and once piece k is done, the outputs below the first
+// output of its successor's first tile are final and are copied on `stream`. That first output is
+// bounded below by the tile's window base, which the host computes from the tile's row (read back
+// once the upper levels are done): no output below the base belongs to a later tile. A BWT byte at
+// x comes from row x or x - 1, so the same bound holds for the BWT.
+constexpr int kMaxDownloadChunks = 8;
+struct OverlappedDownload {
+    uint32_t* sa = nullptr;        // page-locked host outputs (either may be null)
+    uint8_t* bwt = nullptr;
+    const uint32_t* deviceSa = nullptr;  // where the last level writes them
+    const uint8_t* deviceBwt = nullptr;
+    cudaStream_t stream = nullptr;  // the copies' stream
+    cudaEvent_t* events = nullptr;  // kMaxDownloadChunks + 1 events
+    uint32_t* hostRows = nullptr;   // page-locked, 8 * kMaxDownloadChunks words
+    uint64_t outputs = 0;
+};
+
+// The first output any tile from row `r` on can own: the sum of its window starts (planTileWindows).
+inline uint64_t tileOutputBound(const MergeRow& r, const uint32_t* start) {
+    if (r.list == kNoList) return 0;
+    uint64_t sum = 0;
+    for (int b = 0; b < kClasses; b++) {
+        const uint32_t len = start[b + 1] - start[b];
+        const uint32_t c = r.c[b];
+        uint64_t w = static_cast<uint32_t>(b) == r.list ? static_cast<uint64_t>(c) * kMergeG
+                                                         : (c == 0 ? 0 : static_cast<uint64_t>(c - 1) * kMergeG + 1);
+        sum += w < len ? w : len;
+    }
+    return sum;
+}
+
+inline cudaError_t copyDown(const OverlappedDownload& d, uint64_t from, uint64_t to) {
+    if (to <= from) return cudaSuccess;
+    if (d.sa) {
+        SADCS_TRY(cudaMemcpyAsync(d.sa + from, d.deviceSa + from, 4 * (to - from), cudaMemcpyDeviceToHost, d.stream));
+    }
+    if (d.bwt) {
+        SADCS_TRY(cudaMemcpyAsync(d.bwt + from, d.deviceBwt + from, to - from, cudaMemcpyDeviceToHost, d.stream));
+    }
+    return cudaSuccess;
+}
+
 // Merges the class lists of the texts into sa and/or bwt (either may be null). splitters and rows
 // are scratch sized by planMerge; counter is one device word (scratch); rowZero and outBase are per
 // text (rowZero is filled here when a BWT is asked for); rowBase: the class tables' row bases.
@@ -352,7 +400,7 @@ inline cudaError_t mergeClasses(const uint8_t* text, const uint32_t* ranks, cons
                                 uint32_t* counter, uint32_t* hostWord, cudaStream_t stream,
                                 cudaEvent_t finalStart = nullptr, cudaEvent_t finalStop = nullptr,
                                 uint32_t* const* saTexts = nullptr, uint8_t* const* bwtTexts = nullptr,
-                                const uint64_t* carried = nullptr) {
+                                const uint64_t* carried = nullptr, const OverlappedDownload* download = nullptr) {
     MergeLevel level[kMaxLevels];
     for (int L = 0; L <= plan.top; L++) {
         level[L].lists = L == 0 ? lists : splitters + plan.listWord[L];
@@ -389,9 +437,44 @@ inline cudaError_t mergeClasses(const uint8_t* text, const uint32_t* ranks, cons
             args.sa = sa;
             args.bwt = bwt;
             args.carried = carried;
-            if (finalStart) SADCS_TRY(cudaEventRecord(finalStart, stream));
-            SADCS_TRY(launchTree<true>(args, tiles, stream));
-            if (finalStop) SADCS_TRY(cudaEventRecord(finalStop, stream));
+            if (download && (download->sa || download->bwt)) {
+                // In pieces, each piece's final outputs copied down while the next ones run.
+                const int chunks = static_cast<int>(std::min<uint32_t>(kMaxDownloadChunks, args.rowsIn ? tiles : 1));
+                uint32_t first[kMaxDownloadChunks + 1];
+                for (int k = 0; k <= chunks; k++) {
+                    first[k] = static_cast<uint32_t>(static_cast<uint64_t>(tiles) * k / chunks);
+                }
+                for (int k = 1; k < chunks; k++) {
+                    SADCS_TRY(cudaMemcpyAsync(download->hostRows + 8 * (k - 1), args.rowsIn + first[k], sizeof(MergeRow),
+                                              cudaMemcpyDeviceToHost, stream));
+                }
+                SADCS_TRY(cudaEventRecord(download->events[kMaxDownloadChunks], stream));
+                if (finalStart) SADCS_TRY(cudaEventRecord(finalStart, stream));
+                for (int k = 0; k < chunks; k++) {
+                    args.tileOffset = first[k];
+                    SADCS_TRY(launchTree<true>(args, first[k + 1] - first[k], stream));
+                    SADCS_TRY(cudaEventRecord(download->events[k], stream));
+                }
+                if (finalStop) SADCS_TRY(cudaEventRecord(finalStop, stream));
+                SADCS_TRY(cudaEventSynchronize(download->events[kMaxDownloadChunks]));  // the rows are here
+                uint64_t done = 0;
+                for (int k = 0; k < chunks; k++) {
+                    uint64_t end = download->outputs;
+                    if (k + 1 < chunks) {
+                        MergeRow r;
+                        std::memcpy(&r, download->hostRows + 8 * k, sizeof r);
+                        end = std::min<uint64_t>(std::max<uint64_t>(tileOutputBound(r, plan.start[0]), done),
+                                                 download->outputs);
+                    }
+                    SADCS_TRY(cudaStreamWaitEvent(download->stream, download->events[k], 0));
+                    SADCS_TRY(copyDown(*download, done, end));
+                    done = end;
+                }
+            } else {
+                if (finalStart) SADCS_TRY(cudaEventRecord(finalStart, stream));
+                SADCS_TRY(launchTree<true>(args, tiles, stream));
+                if (finalStop) SADCS_TRY(cudaEventRecord(finalStop, stream));
+            }
         } else {
             args.rowsOut = rows + plan.rowIndex[L - 1];
             SADCS_TRY(launch(mergeWriteSentinel, 1, 32, 0, stream, rows + plan.rowIndex[L - 1] + plan.tiles[L - 1],

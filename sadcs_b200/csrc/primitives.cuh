@@ -368,7 +368,7 @@ struct SortTilesPerSm<Loader, std::void_t<decltype(Loader::kTilesPerSm)>> {
 #endif
 // Carrying passes in mode 1 store their values from the threads too, beside the words (a warp's
 // stores fall into one run per digit: few digits in the carrying passes), without staging them by
-// slot (tuning).
+// slot (tuning: class phase of the 3 GiB genome-like text 75.7 ms against 74.2 staged).
 #ifndef SADCS_CARRY_DIRECT_VALUES
 #define SADCS_CARRY_DIRECT_VALUES 0
 #endif

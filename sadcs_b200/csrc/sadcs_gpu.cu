@@ -320,6 +320,8 @@ struct sadcs_gpu_context {
     uint32_t* hostWords = nullptr;  // page-locked: counters and the per-construction tables
     size_t hostWordCount = 0;
     cudaEvent_t events[6] = {};
+    cudaStream_t copyStream = nullptr;  // the outputs' copies to page-locked host buffers during the merge
+    cudaEvent_t chunkEvents[kMaxDownloadChunks + 1] = {};
 };
 
 namespace {
@@ -330,9 +332,14 @@ void destroyContext(sadcs_gpu_context* c) {
     cudaGetDevice(&previous);
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->copyStream) cudaStreamSynchronize(c->copyStream);
     for (cudaEvent_t& e : c->events) {
         if (e) cudaEventDestroy(e);
     }
+    for (cudaEvent_t& e : c->chunkEvents) {
+        if (e) cudaEventDestroy(e);
+    }
+    if (c->copyStream) cudaStreamDestroy(c->copyStream);
     if (c->stream) cudaStreamDestroy(c->stream);
     if (c->slab) cudaFree(c->slab);
     if (c->hostWords) cudaFreeHost(c->hostWords);
@@ -423,6 +430,18 @@ int createContext(int64_t capacity, uint32_t texts, sadcs_gpu_context** out) {
         destroyContext(c);
         return status;
     }
+    if ((error = cudaStreamCreateWithFlags(&c->copyStream, cudaStreamNonBlocking)) != cudaSuccess) {
+        const int status = failed("creating the context", error);
+        destroyContext(c);
+        return status;
+    }
+    for (cudaEvent_t& e : c->chunkEvents) {
+        if ((error = cudaEventCreateWithFlags(&e, cudaEventDisableTiming)) != cudaSuccess) {
+            const int status = failed("cudaEventCreate", error);
+            destroyContext(c);
+            return status;
+        }
+    }
     for (cudaEvent_t& e : c->events) {
         if ((error = cudaEventCreate(&e)) != cudaSuccess) {
             const int status = failed("cudaEventCreate", error);
@@ -507,6 +526,8 @@ struct Io {
     bool wantSa = false, wantBwt = false;
     uint32_t* outSa = nullptr;            // device outputs (caller-owned), or null for the slab's
     uint8_t* outBwt = nullptr;
+    uint32_t* hostSa = nullptr;           // page-locked host outputs, copied down from the slab's while
+    uint8_t* hostBwt = nullptr;           // the last merge level runs (context copy stream)
     // results
     uint32_t* deviceSa = nullptr;         // where the SA / BWT ended up
     uint8_t* deviceBwt = nullptr;
@@ -703,13 +724,28 @@ int construct(sadcs_gpu_context* c, const Batch& b, Io& io, cudaStream_t stream,
     uint8_t* bwt = bwtPieces ? nullptr : (io.outBwt ? io.outBwt : (io.wantBwt ? slab + L.bwt : nullptr));
     // The merge's tile shape follows the code width, known now (the memory plan bounds every shape).
     const MergePlan mergePlan = planMerge(b.classes.start, mergeR(finalWords(texts.bits)));
+    OverlappedDownload download;
+    const bool overlapped = (io.hostSa || io.hostBwt) && c->copyStream;
+    if (overlapped) {
+        download.sa = io.hostSa;
+        download.bwt = io.hostBwt;
+        download.deviceSa = sa;
+        download.deviceBwt = bwt;
+        download.stream = c->copyStream;
+        download.events = c->chunkEvents;
+        download.hostRows = c->hostWords + 64;  // the tables' staging words, free since their upload
+        download.outputs = b.outputs;
+    }
     if ((error = mergeClasses(text, ranks, texts, lists, mergePlan, classTables.rowBase, dOutBase, dRowZero,
                               reinterpret_cast<uint32_t*>(slab + L.splitters),
                               reinterpret_cast<MergeRow*>(slab + L.rows), sa, bwt,
                               reinterpret_cast<uint32_t*>(slab + L.mergeCounter), c->hostWords, stream,
-                              c->events[4], c->events[5], saPieces, bwtPieces, carried)) != cudaSuccess) {
+                              c->events[4], c->events[5], saPieces, bwtPieces, carried,
+                              overlapped ? &download : nullptr)) != cudaSuccess) {
+        if (overlapped) cudaStreamSynchronize(c->copyStream);
         return failed("merge", error);
     }
+    if (overlapped && (error = cudaStreamSynchronize(c->copyStream)) != cudaSuccess) return failed("download", error);
     cudaEventRecord(c->events[3], stream);
     if ((error = cudaStreamSynchronize(stream)) != cudaSuccess) return failed("merge", error);
     s.merge_seconds = secondsSince(start);
@@ -750,6 +786,18 @@ int withContext(sadcs_gpu_context* context, uint64_t total, uint32_t texts, sadc
     destroyContext(temporary);
     s.setup_seconds = setup;
     return status;
+}
+
+// How page-locked host outputs are filled: copied down in pieces while the last merge level runs
+// (the default), written by the last merge level itself through their device mapping, or copied
+// down after the construction. The environment's SADCS_HOST_OUTPUTS ("overlapped", "mapped",
+// "after") overrides the default, read at each call (tests and tuning).
+enum class HostOutputs { Overlapped, Mapped, After };
+HostOutputs hostOutputMode() {
+    const char* v = std::getenv("SADCS_HOST_OUTPUTS");
+    if (v && std::strcmp(v, "mapped") == 0) return HostOutputs::Mapped;
+    if (v && std::strcmp(v, "after") == 0) return HostOutputs::After;
+    return HostOutputs::Overlapped;
 }
 
 int download(sadcs_gpu_context* c, void* host, const void* device, size_t bytes, sadcs_gpu_stats& s) {
@@ -886,14 +934,26 @@ int sadcs_gpu_build_batch(sadcs_gpu_context* context, const uint8_t* texts, cons
         io.hostText = texts;
         io.wantSa = sa != nullptr;
         io.wantBwt = bwt != nullptr;
-        // Page-locked outputs are written by the merge itself, over the host link while it runs,
-        // instead of being copied down after it.
-        io.outSa = static_cast<uint32_t*>(mappedHost(sa));
-        io.outBwt = static_cast<uint8_t*>(mappedHost(bwt));
+        // Page-locked outputs are copied down piece by piece while the last merge level runs (or
+        // written by the merge itself over the host link, or copied after it: hostOutputMode).
+        const HostOutputs mode = hostOutputMode();
+        uint32_t* mappedSa = static_cast<uint32_t*>(mappedHost(sa));
+        uint8_t* mappedBwt = static_cast<uint8_t*>(mappedHost(bwt));
+        if (mode == HostOutputs::Mapped) {
+            io.outSa = mappedSa;
+            io.outBwt = mappedBwt;
+        } else if (mode == HostOutputs::Overlapped && c->copyStream) {
+            io.hostSa = mappedSa ? sa : nullptr;
+            io.hostBwt = mappedBwt ? bwt : nullptr;
+        }
         int status = construct(c, b, io, c->stream, s);
         if (status != SADCS_OK) return status;
-        if (sa && !io.outSa && (status = download(c, sa, io.deviceSa, 4 * b.outputs, s)) != SADCS_OK) return status;
-        if (bwt && !io.outBwt && (status = download(c, bwt, io.deviceBwt, b.outputs, s)) != SADCS_OK) return status;
+        if (sa && !io.outSa && !io.hostSa && (status = download(c, sa, io.deviceSa, 4 * b.outputs, s)) != SADCS_OK) {
+            return status;
+        }
+        if (bwt && !io.outBwt && !io.hostBwt && (status = download(c, bwt, io.deviceBwt, b.outputs, s)) != SADCS_OK) {
+            return status;
+        }
         if (bwt && primaries) {
             std::vector<int64_t> p(b.count);
             if ((status = readPrimaries(c, io, b.count, p.data())) != SADCS_OK) return status;

@@ -271,20 +271,35 @@ def test_server_results_equal_alone_and_in_the_mix():
         assert 0 < constructions < len(texts) and launches > 0
 
 
+@pytest.mark.parametrize("mode", ["overlapped", "mapped", "after"])
 @pytest.mark.parametrize("n", [1, 2, 100, 70000, 3 << 20])
-def test_page_locked_outputs_written_by_the_device(n):
-    """With page-locked output buffers the merge writes the SA and BWT into host memory directly;
-    the results equal those of the pageable path."""
-    text = W.natural_text(n, seed=31) if n > 100 else W.random_text(W.SplitMix(n), n, 3)
-    ref_sa, ref_bwt, ref_primary = sa.build(text)
+def test_page_locked_outputs(n, mode, monkeypatch):
+    """Page-locked output buffers: copied down piece by piece while the last merge level runs (the
+    default: each piece up to the window base of the next piece's first tile), written by the merge
+    itself through their device mapping, or copied after the construction. The results equal those
+    of the pageable path, for natural-language-like text and for DNA-like text with carried words
+    (pieces of SA only, BWT only, and both)."""
+    rng = W.SplitMix(n)
+    texts = [W.natural_text(n, seed=31) if n > 100 else W.random_text(rng, n, 3), W.random_text(rng, n, 4)]
+    monkeypatch.setenv("SADCS_CARRY_MIN_BYTES", "0")
     raw_sa = sa.allocate_pinned(4 * n)
     raw_bwt = sa.allocate_pinned(n)
     try:
-        out_sa = raw_sa.view(np.uint32)
-        out_sa[:] = 0xFFFFFFFF
-        raw_bwt[:] = 0
-        got_sa, got_bwt, primary = sa.build(text, out_sa=out_sa, out_bwt=raw_bwt)
-        assert np.array_equal(got_sa, ref_sa) and np.array_equal(got_bwt, ref_bwt) and primary == ref_primary
+        for text in texts:
+            monkeypatch.setenv("SADCS_HOST_OUTPUTS", "after")
+            ref_sa, ref_bwt, ref_primary = sa.build(text)
+            monkeypatch.setenv("SADCS_HOST_OUTPUTS", mode)
+            out_sa = raw_sa.view(np.uint32)
+            for want_sa, want_bwt in ((True, True), (True, False), (False, True)):
+                out_sa[:] = 0xFFFFFFFF
+                raw_bwt[:] = 0
+                got_sa, got_bwt, primary = sa.build(text, want_sa=want_sa, want_bwt=want_bwt,
+                                                    out_sa=out_sa if want_sa else None,
+                                                    out_bwt=raw_bwt if want_bwt else None)
+                if want_sa:
+                    assert np.array_equal(got_sa, ref_sa), f"{mode}: SA differs (n={n})"
+                if want_bwt:
+                    assert np.array_equal(got_bwt, ref_bwt) and primary == ref_primary, f"{mode}: BWT differs (n={n})"
     finally:
         sa.free_pinned(raw_sa)
         sa.free_pinned(raw_bwt)
