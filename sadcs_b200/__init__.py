@@ -315,16 +315,21 @@ def required_bytes_batch(total: int, texts: int) -> int:
 
 
 def build_batch(texts, want_sa: bool = True, want_bwt: bool = True, context: Context | None = None,
-                stats: Stats | None = None):
-    """SA and/or BWT of every text of a list in one construction (sadcs_gpu_build_batch).
+                stats: Stats | None = None, out_sa: np.ndarray | None = None, out_bwt: np.ndarray | None = None):
+    """SA and/or BWT of every text of a list in one construction (sadcs_gpu_build_batch). out_sa /
+    out_bwt may be given as the output buffers of all texts one after another (page-locked ones are
+    filled while the construction runs).
 
     Returns (list of SA arrays or None, list of BWT arrays or None, list of primaries or None)."""
     arrays = [_as_text(t) for t in texts]
     lengths = np.array([len(a) for a in arrays], dtype=np.int64)
     packed = np.ascontiguousarray(np.concatenate(arrays) if arrays else np.zeros(0, np.uint8))
     total = int(lengths.sum())
-    sa = np.empty(max(total, 1), np.uint32) if want_sa else None
-    out = np.empty(max(total, 1), np.uint8) if want_bwt else None
+    sa = (out_sa if out_sa is not None else np.empty(max(total, 1), np.uint32)) if want_sa else None
+    out = (out_bwt if out_bwt is not None else np.empty(max(total, 1), np.uint8)) if want_bwt else None
+    if (sa is not None and (sa.dtype != np.uint32 or len(sa) < total)) or (
+            out is not None and (out.dtype != np.uint8 or len(out) < total)):
+        raise ValueError("out_sa must be uint32 and out_bwt uint8, each of at least the texts' total length")
     primaries = np.zeros(max(len(arrays), 1), np.int64)
     _check(lib().sadcs_gpu_build_batch(_handle(context), packed.ctypes.data_as(_u8p) if packed.size else None,
                                        lengths.ctypes.data_as(_i64p), len(arrays),

@@ -305,6 +305,30 @@ def test_page_locked_outputs(n, mode, monkeypatch):
         sa.free_pinned(raw_bwt)
 
 
+@pytest.mark.parametrize("mode", ["overlapped", "mapped", "after"])
+def test_page_locked_outputs_of_a_batch(mode, monkeypatch):
+    """A batch of uneven texts into page-locked buffers (all texts one after another): the pieces
+    copied down while the last merge level runs follow the global output order across texts; every
+    text's SA, BWT and primary equal its own construction's."""
+    monkeypatch.setenv("SADCS_HOST_OUTPUTS", mode)
+    texts = W.batch_texts(60, lo=1 << 8, hi=1 << 18, seed=22) + [W.natural_text(1 << 20, seed=23)]
+    total = sum(len(t) for t in texts)
+    raw_sa = sa.allocate_pinned(4 * total)
+    raw_bwt = sa.allocate_pinned(total)
+    try:
+        out_sa = raw_sa.view(np.uint32)
+        out_sa[:] = 0xFFFFFFFF
+        raw_bwt[:] = 0
+        sas, bwts, primaries = sa.build_batch(texts, out_sa=out_sa, out_bwt=raw_bwt)
+        for k, t in enumerate(texts):
+            es, eb, ep = _expected(t)
+            assert np.array_equal(sas[k], es) and np.array_equal(bwts[k], eb) and primaries[k] == ep, \
+                f"{mode}: text {k} differs"
+    finally:
+        sa.free_pinned(raw_sa)
+        sa.free_pinned(raw_bwt)
+
+
 def test_server_page_locked_outputs_in_batches():
     """Requests whose outputs are page-locked: the batched merge writes each request's SA and BWT
     into that request's own buffers; every result equals its text built alone."""
