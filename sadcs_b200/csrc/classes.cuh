@@ -255,14 +255,8 @@ struct ClassLoader {
         if (k == 0) return carriedWord(texts.packed, texts.endOfText(j) - 1, texts.bits);
         return carried[__ldg(prevOffset + j) + k - 1];
     }
-    __device__ __forceinline__ const uint64_t* carrySourceAt(uint32_t j, uint32_t, uint32_t k) const {
-        return k == 0 ? nullptr : carried + __ldg(prevOffset + j) + k - 1;
-    }
-    __device__ __forceinline__ uint64_t carryCombine(uint32_t tag, uint64_t source) const {
-        return (static_cast<uint64_t>(tag) << (64 - texts.bits)) | (source >> texts.bits);
-    }
     __device__ __forceinline__ uint64_t carryWord(uint32_t k, uint32_t tag, uint64_t source) const {
-        return k == 0 ? source : carryCombine(tag, source);
+        return k == 0 ? source : (static_cast<uint64_t>(tag) << (64 - texts.bits)) | (source >> texts.bits);
     }
 };
 

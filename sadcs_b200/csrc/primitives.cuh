@@ -293,14 +293,12 @@ constexpr long long kLookbackLimitCycles = 4000000000ll;
 
 // Shared memory of radixOnesweep for a key of keyBytes bytes: one staging buffer that holds the
 // tile's keys, then its values, then (carry mode 0) its 64-bit carried words; the digit of every
-// staged slot, (carry) a tag byte per slot, the counting tables, and (carry mode 3) a buffer of the
-// carried words' sources by slot. The shared memory a block does not take is L1.
+// staged slot, (carry) a tag byte per slot, and the counting tables. The shared memory a block does
+// not take is L1.
 constexpr size_t radixSharedBytes(size_t keyBytes, bool carry = false, int carryMode = 0) {
     const size_t stage = carry && carryMode == 0 ? 8 : (keyBytes > 4 ? keyBytes : 4);
-    return kSortTile * stage + kSortTile * (carry ? 2 : 1) + (kSortWarps * 256 + 256 + 256 + 32) * 4 +
-           (carry && carryMode == 3 ? 8 * kSortTile : 0) + 64;
+    return kSortTile * stage + kSortTile * (carry ? 2 : 1) + (kSortWarps * 256 + 256 + 256 + 32) * 4 + 64;
 }
-constexpr uint8_t kCarryAsIs = 0xFF;  // tag of a slot whose source is its carried word already
 
 // Segments of a pass: element ranges sorted independently, each from its own digit bases, with
 // tiles that never span two segments. The one-segment case is the plain sort.
@@ -356,21 +354,16 @@ struct SortTilesPerSm<Loader, std::void_t<decltype(Loader::kTilesPerSm)>> {
 // A loader may carry a 64-bit word with every element (kCarry): it gives a tag byte from the key
 // (carryTag), staged while the key is in registers, a source word read by the element's index
 // (carrySource), and the element's carried word from the two (carryWord); the storer writes it
-// (storeCarry). SADCS_CARRY_MODE: 0 reads the sources after the look-back and stages the words by
-// slot (whole-run stores); 1 reads them after the look-back and stores each from its thread (a
-// warp's stores fall into one run per digit); 2 as 1, but with the sources read before the
-// look-back, with the values; 3 copies the sources asynchronously into a slot-ordered buffer of
-// their own before the look-back (carrySourceAt; no registers held), then stores in runs (tuning).
-// Measured on the 3 GiB genome-like text (class phase): mode 0 91.3 ms, 1 82.8, 2 93.8 (3 tiles per
-// SM: its registers spill at 4), 3 95.6 (3 tiles per SM: its shared memory).
+// (storeCarry). The sources are read after the look-back, all in flight at once. SADCS_CARRY_MODE:
+// 1 stores each word from its thread (a warp's stores fall into one run per digit: few digits in
+// the carrying passes); 0 stages the words by slot for whole-run stores (tuning). Measured on the
+// 3 GiB genome-like text (class phase): mode 1 82.8 ms, mode 0 91.3; the sources read before the
+// look-back, with the values, 93.8 (3 tiles per SM: the registers spill at 4); the sources copied
+// asynchronously into a slot-ordered shared buffer before the look-back 95.6 (3 tiles per SM: its
+// 32 KB); mode 1 with the values also stored from the threads, unstaged, 75.7 against 74.2 (with
+// the later class-0 changes).
 #ifndef SADCS_CARRY_MODE
 #define SADCS_CARRY_MODE 1
-#endif
-// Carrying passes in mode 1 store their values from the threads too, beside the words (a warp's
-// stores fall into one run per digit: few digits in the carrying passes), without staging them by
-// slot (tuning: class phase of the 3 GiB genome-like text 75.7 ms against 74.2 staged).
-#ifndef SADCS_CARRY_DIRECT_VALUES
-#define SADCS_CARRY_DIRECT_VALUES 0
 #endif
 template <class Loader, class = void>
 struct LoaderCarries {
@@ -391,9 +384,6 @@ __global__ void __launch_bounds__(kSortThreads, SortTilesPerSm<Loader>::value) r
     extern __shared__ __align__(16) unsigned char smem[];
     constexpr bool kCarry = LoaderCarries<Loader>::value;
     constexpr bool kStageCarry = kCarry && SADCS_CARRY_MODE == 0;
-    constexpr bool kEarlyCarry = kCarry && SADCS_CARRY_MODE == 2;
-    constexpr bool kPrefetchCarry = kCarry && SADCS_CARRY_MODE == 3;
-    constexpr bool kDirectValues = kCarry && SADCS_CARRY_MODE == 1 && SADCS_CARRY_DIRECT_VALUES;
     constexpr size_t kStageBytes = kSortTile * (kStageCarry ? 8 : (sizeof(Key) > 4 ? sizeof(Key) : 4));
     Key* sKeys = reinterpret_cast<Key*>(smem);
     uint32_t* sVals = reinterpret_cast<uint32_t*>(smem);  // the same buffer, after the keys are out
@@ -404,7 +394,6 @@ __global__ void __launch_bounds__(kSortThreads, SortTilesPerSm<Loader>::value) r
     uint32_t* digitStart = warpCount + kSortWarps * 256;
     uint32_t* digitGlobal = digitStart + 256;
     uint32_t* warpTotals = digitGlobal + 256;
-    uint64_t* sSource = reinterpret_cast<uint64_t*>(warpTotals + 32);  // prefetch mode only (16-byte aligned)
     __shared__ uint32_t sTile;
     __shared__ int sFailed;
 
@@ -471,12 +460,10 @@ __global__ void __launch_bounds__(kSortThreads, SortTilesPerSm<Loader>::value) r
     // Stage the keys (and every slot's digit) by digit before the look-back, so that the keys leave
     // the registers, and start the value loads, which complete while the look-back waits.
     uint32_t vals[kSortItems];
-    uint64_t sources[kCarry ? kSortItems : 1];
 #pragma unroll
     for (int j = 0; j < kSortItems; j++) {
         const uint32_t dj = rankDigit[j] & 0x1FF;
         vals[j] = 0;
-        if constexpr (kEarlyCarry) sources[j] = 0;
         if (dj != kNoDigit) {
             const uint32_t slot = digitStart[dj] + warpCount[warp * 256 + dj] + (rankDigit[j] >> 9);
             if constexpr (Storer::kKeys) sKeys[slot] = keys[j];
@@ -485,18 +472,6 @@ __global__ void __launch_bounds__(kSortThreads, SortTilesPerSm<Loader>::value) r
             rankDigit[j] = slot;  // from here on: the item's staged slot
             const uint64_t i = warpBase + j * 32 + lane;
             vals[j] = ld.value(segment, segBegin + static_cast<uint32_t>(i), static_cast<uint32_t>(i));
-            if constexpr (kEarlyCarry) {
-                sources[j] = ld.carrySource(segment, segBegin + static_cast<uint32_t>(i), static_cast<uint32_t>(i));
-            }
-            if constexpr (kPrefetchCarry) {
-                const uint64_t* from = ld.carrySourceAt(segment, segBegin + static_cast<uint32_t>(i), static_cast<uint32_t>(i));
-                if (from) {
-                    cpAsync8(sSource + slot, from);
-                } else {
-                    sSource[slot] = ld.carrySource(segment, segBegin + static_cast<uint32_t>(i), static_cast<uint32_t>(i));
-                    sTag[slot] = kCarryAsIs;
-                }
-            }
         } else {
             rankDigit[j] = 0xFFFFFFFFu;
         }
@@ -550,41 +525,10 @@ __global__ void __launch_bounds__(kSortThreads, SortTilesPerSm<Loader>::value) r
     digitGlobal[d] = digitBase[static_cast<size_t>(segment) * 256 + d] + exclusive;
     __syncthreads();
     if (sFailed) {
-        if constexpr (kPrefetchCarry) cpAsyncWaitAll();  // no copy into shared memory outlives the block
         if (threadIdx.x == 0) atomicExch(error, 1u);
         return;
     }
 
-    if constexpr (kDirectValues) {
-        // Sources of the carried words first (every read in flight), then the keys in runs and each
-        // item's value and word from its thread.
-#pragma unroll
-        for (int j = 0; j < kSortItems; j++) {
-            const uint64_t i = warpBase + j * 32 + lane;
-            sources[j] = 0;
-            if (rankDigit[j] != 0xFFFFFFFFu) {
-                sources[j] = ld.carrySource(segment, segBegin + static_cast<uint32_t>(i), static_cast<uint32_t>(i));
-            }
-        }
-        if constexpr (Storer::kKeys) {
-            for (uint32_t i = threadIdx.x; i < tileTotal; i += kSortThreads) {
-                const uint32_t dj = sDig[i];
-                st.storeKey(segment, digitGlobal[dj] + i - digitStart[dj], sKeys[i]);
-            }
-        }
-#pragma unroll
-        for (int j = 0; j < kSortItems; j++) {
-            const uint32_t slot = rankDigit[j];
-            if (slot != 0xFFFFFFFFu) {
-                const uint64_t i = warpBase + j * 32 + lane;
-                const uint32_t dj = sDig[slot];
-                const uint32_t pos = digitGlobal[dj] + slot - digitStart[dj];
-                st.storeValue(segment, pos, vals[j]);
-                st.storeCarry(segment, pos, ld.carryWord(static_cast<uint32_t>(i), sTag[slot], sources[j]));
-            }
-        }
-        return;
-    }
     if constexpr (Storer::kKeys) {
         for (uint32_t i = threadIdx.x; i < tileTotal; i += kSortThreads) {
             const uint32_t dj = sDig[i];
@@ -602,27 +546,16 @@ __global__ void __launch_bounds__(kSortThreads, SortTilesPerSm<Loader>::value) r
         const uint32_t dj = sDig[i];
         st.storeValue(segment, digitGlobal[dj] + i - digitStart[dj], sVals[i]);
     }
-    if constexpr (kPrefetchCarry) {
-        cpAsyncWaitAll();
-        __syncthreads();
-        for (uint32_t i = threadIdx.x; i < tileTotal; i += kSortThreads) {
-            const uint32_t dj = sDig[i];
-            const uint8_t tag = sTag[i];
-            const uint64_t source = sSource[i];
-            st.storeCarry(segment, digitGlobal[dj] + i - digitStart[dj],
-                          tag == kCarryAsIs ? source : ld.carryCombine(tag, source));
-        }
-    } else if constexpr (kCarry) {
+    if constexpr (kCarry) {
         // The carried words: sources read in element order (every read in flight), then each word
-        // staged by slot and written in runs (mode 0) or written from its thread (modes 1, 2).
-        if constexpr (!kEarlyCarry) {
+        // staged by slot and written in runs (mode 0) or written from its thread (mode 1).
+        uint64_t sources[kSortItems];
 #pragma unroll
-            for (int j = 0; j < kSortItems; j++) {
-                const uint64_t i = warpBase + j * 32 + lane;
-                sources[j] = 0;
-                if (rankDigit[j] != 0xFFFFFFFFu) {
-                    sources[j] = ld.carrySource(segment, segBegin + static_cast<uint32_t>(i), static_cast<uint32_t>(i));
-                }
+        for (int j = 0; j < kSortItems; j++) {
+            const uint64_t i = warpBase + j * 32 + lane;
+            sources[j] = 0;
+            if (rankDigit[j] != 0xFFFFFFFFu) {
+                sources[j] = ld.carrySource(segment, segBegin + static_cast<uint32_t>(i), static_cast<uint32_t>(i));
             }
         }
         if constexpr (kStageCarry) {
