@@ -72,3 +72,13 @@ extern "C" uint64_t plan_peak(const uint64_t* lengths, uint32_t count) {
     if (!planBatch(lengths, count, b)) return 0;
     return planLayout(extentOf(b), true, true, planCarry(b.outputs, count)).peak;
 }
+
+// The first output any tile from this row on can own (merge.cuh: tileOutputBound, the bound the
+// overlapped download of the last merge level copies up to). row: list (or -1 for the level's
+// start) then 7 counts; start: the 8 list offsets of the level.
+extern "C" uint64_t plan_tile_bound(const uint32_t* row, const uint32_t* start) {
+    MergeRow r;
+    r.list = row[0];
+    for (int b = 0; b < kClasses; b++) r.c[b] = row[1 + b];
+    return tileOutputBound(r, start);
+}

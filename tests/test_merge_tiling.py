@@ -3,7 +3,9 @@ above), restated in numpy: for any interleaving of the 7 sorted class lists, eve
 fits the fixed shared-memory capacity G*R + 6*(G-1) + 1, the windows hold every element the tile
 outputs, and an element's output index (the windows' total start plus its rank among them) is its
 position in the merged order. The kernel has no overflow path, so this bound is what keeps it in
-bounds whatever the text."""
+bounds whatever the text. Also the bound the overlapped download of the last level relies on: no
+output below a tile's window base comes from that tile or a later one (its C++ form, tileOutputBound,
+through tests/plan_harness.cu)."""
 import numpy as np
 import pytest
 
@@ -63,6 +65,7 @@ def check_tiling(lists, R):
     values = np.sort(np.concatenate(lists))
     rows = rows_of_level_above(lists, R)
     written = np.zeros(len(values), dtype=np.int64)
+    starts = []  # (window base, first output) of every tile
     for t in range(len(rows) - 1):
         lo, hi = rows[t], rows[t + 1]
         w, e = windows(lo, hi, lens)
@@ -83,7 +86,14 @@ def check_tiling(lists, R):
             pos = base + r
             assert values[pos] == window[r]
             written[pos] += 1
+        starts.append((base, base + first))
     assert np.all(written == 1)
+    # Tiles own consecutive output ranges in tile order, each starting at or above its window base:
+    # once tiles [0, t) are done, every output below tile t's base is final.
+    for t, (base, first_out) in enumerate(starts):
+        assert base <= first_out, (t, base, first_out)
+        assert t == 0 or starts[t - 1][1] <= first_out
+    return rows, starts
 
 
 def class_sized_lists(rng, n, assign):
@@ -150,3 +160,26 @@ def test_tiles_with_empty_and_tiny_lists():
         for R in (40, 80):
             check_tiling(lists, R)
 
+
+def test_tile_output_bound_matches_the_library():
+    """tileOutputBound (merge.cuh, host code) gives each tile's window base, as restated above."""
+    from tests.test_memory_plan import harness
+
+    lib = harness()
+    import ctypes
+
+    lib.plan_tile_bound.restype = ctypes.c_uint64
+    lib.plan_tile_bound.argtypes = [ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint32)]
+    rng = np.random.default_rng(8)
+    for assign in (random_assign, block_assign, comb_assign):
+        for n in (3000, 100000):
+            lists = class_sized_lists(rng, n, assign)
+            lens = [len(l) for l in lists]
+            start = np.concatenate([[0], np.cumsum(lens)]).astype(np.uint32)
+            rows, starts = check_tiling(lists, 40)
+            for t in range(len(rows) - 1):
+                lo = rows[t]
+                row = np.array([0xFFFFFFFF if lo[0] is None else lo[0], *lo[1]], dtype=np.uint32)
+                got = lib.plan_tile_bound(row.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)),
+                                          start.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)))
+                assert got == starts[t][0], (t, got, starts[t][0])
