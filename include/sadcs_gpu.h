@@ -88,7 +88,9 @@ int64_t sadcs_gpu_sample_size(int64_t n);
 /* gpuQueryDevice, gpusa.h:76: the current CUDA device and its memory. */
 int sadcs_gpu_query_device(sadcs_gpu_device* device);
 
-/* gpuRequiredBytes, gpusa.h:79: peak device memory of a construction of n bytes, -1 if n is out of range. */
+/* gpuRequiredBytes, gpusa.h:79: peak device memory of a construction of n bytes, -1 if n is out of
+ * range: about 11n, and 19n from the carry threshold on (256 MiB, or SADCS_CARRY_MIN_BYTES), where a
+ * one-text context keeps room for the code words its class passes hand to the merge. */
 int64_t sadcs_gpu_required_bytes(int64_t n);
 
 /* gpuCreateContext, gpusa.h:93: device memory for inputs of up to capacity bytes, reserved once.
