@@ -393,7 +393,8 @@ size_t contextBytes(int64_t capacity, uint32_t texts) {
     return contextBytes(capacity, texts, planCarry(static_cast<uint64_t>(capacity), texts));
 }
 
-int createContext(int64_t capacity, uint32_t texts, sadcs_gpu_context** out) {
+// carryRoom false: no room for carried words whatever the size (callers that never construct).
+int createContext(int64_t capacity, uint32_t texts, sadcs_gpu_context** out, bool carryRoom = true) {
     *out = nullptr;
     sadcs_gpu_device device;
     if (const int status = queryDevice(&device); status != SADCS_OK) return status;
@@ -402,7 +403,7 @@ int createContext(int64_t capacity, uint32_t texts, sadcs_gpu_context** out) {
                  static_cast<long long>(capacity), texts, static_cast<long long>(kMaxText), kMaxTexts);
         return SADCS_FAILED;
     }
-    const bool carry = planCarry(static_cast<uint64_t>(capacity), texts);
+    const bool carry = carryRoom && planCarry(static_cast<uint64_t>(capacity), texts);
     const size_t bytes = contextBytes(capacity, texts, carry);
     if (static_cast<int64_t>(bytes) + kMemoryReserve > device.free_bytes) {
         setError("needs %lld MiB of device memory plus %lld MiB reserve, %lld MiB free",
@@ -766,7 +767,8 @@ int construct(sadcs_gpu_context* c, const Batch& b, Io& io, cudaStream_t stream,
 // Runs body(context) with the given context, or a temporary one for `total` bytes in `texts` texts
 // (its creation is setup).
 template <class Body>
-int withContext(sadcs_gpu_context* context, uint64_t total, uint32_t texts, sadcs_gpu_stats& s, Body body) {
+int withContext(sadcs_gpu_context* context, uint64_t total, uint32_t texts, sadcs_gpu_stats& s, Body body,
+                bool carryRoom = true) {
     if (context) {
         int previous = 0;
         cudaGetDevice(&previous);
@@ -777,7 +779,8 @@ int withContext(sadcs_gpu_context* context, uint64_t total, uint32_t texts, sadc
     }
     const auto start = std::chrono::steady_clock::now();
     sadcs_gpu_context* temporary = nullptr;
-    if (const int status = createContext(static_cast<int64_t>(total), texts, &temporary); status != SADCS_OK) {
+    if (const int status = createContext(static_cast<int64_t>(total), texts, &temporary, carryRoom);
+        status != SADCS_OK) {
         return status;
     }
     s.setup_seconds = secondsSince(start);
@@ -1557,7 +1560,7 @@ int sadcs_gpu_rank_sample(const uint8_t* text, int64_t n, uint32_t* ranks, sadcs
         s.ranking_bytes = static_cast<int64_t>(L.rankingEnd);
         s.device_bytes = s.ranking_bytes;
         return download(c, ranks, rankBuffer, 4 * b.live, s);
-    });
+    }, /*carryRoom=*/false);  // ranking only: no class passes
 }
 
 void* sadcs_gpu_allocate_pinned(size_t bytes) {

@@ -329,6 +329,37 @@ def test_page_locked_outputs_of_a_batch(mode, monkeypatch):
         sa.free_pinned(raw_bwt)
 
 
+def test_server_carried_words(monkeypatch):
+    """Requests built alone by the server (one text per construction) with carried words forced on
+    (normally from 256 MiB on): the server plans the room for them in a request's footprint and its
+    construction uses it; results equal the oracle's, pageable and page-locked outputs alike."""
+    monkeypatch.setenv("SADCS_CARRY_MIN_BYTES", "0")
+    rng = W.SplitMix(24)
+    texts = [W.random_text(rng, n, 4) for n in (1000, 70000, 1 << 20)] + [W.genome_text(1 << 21, seed=7),
+                                                                             W.random_text(rng, 5000, 2)]
+    raw = sa.allocate_pinned(sum(5 * len(t) + 64 for t in texts))
+    try:
+        with sa.Server(workers=2, small_limit=1 << 20, batch_bytes=64 << 20, batch_texts=1) as server:
+            tickets, at = [], 0
+            for k, t in enumerate(texts):
+                n = len(t)
+                if k % 2:
+                    out_sa = raw[at:at + 4 * n].view(np.uint32)
+                    at += (4 * n + 15) // 16 * 16
+                    out_bwt = raw[at:at + n]
+                    at += (n + 15) // 16 * 16
+                    tickets.append(server.submit(t, sa=out_sa, bwt=out_bwt))
+                else:
+                    tickets.append(server.submit(t))
+            for k, ticket in enumerate(tickets):
+                s_, b_, p_, _, size = server.wait(ticket)
+                es, eb, ep = _expected(texts[k])
+                assert size == 1
+                assert np.array_equal(s_, es) and np.array_equal(b_, eb) and p_ == ep, f"request {k} differs"
+    finally:
+        sa.free_pinned(raw)
+
+
 def test_server_page_locked_outputs_in_batches():
     """Requests whose outputs are page-locked: the batched merge writes each request's SA and BWT
     into that request's own buffers; every result equals its text built alone."""
